@@ -1,0 +1,434 @@
+"""B200 (sm_100a) Fokker-Planck propagation on SO(3) x R^n.
+
+Host-side mirror of the reference's MEX / MATLAB interface for the propagation
+path (fdcl-gwu/hybridPendulum-UP): the functions below keep the reference's
+names, argument order and array layouts, and call the CUDA library ``libhp.so``
+through its C ABI (``include/hp.h``).  There is no CPU fallback: importing this
+package fails if the library has not been built (``python build.py``).
+
+Arrays are numpy (host, staged through the plan) or torch CUDA tensors
+(device pointers, no copies).  Layouts are the MATLAB column-major ones:
+    F  (2lmax+1, 2lmax+1, lmax+1, 2Bx, 2Bx[, 2Bx]) complex128
+    f  (2B, 2B, 2B, 2Bx, 2Bx[, 2Bx])                float64 (complex128 for complex plans)
+so a C-ordered numpy array of the reversed shape, or an F-ordered array of the
+MATLAB shape, is passed as is.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from functools import lru_cache
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, 'libhp.so')
+
+HP_OK, HP_ERR_INVALID, HP_ERR_SHAPE, HP_ERR_ALLOC, HP_ERR_CUDA = 0, 1, 2, 3, 4
+HP_ERR_UNSUPPORTED, HP_ERR_NONFINITE, HP_ERR_NO_MODEL = 5, 6, 7
+HP_FP64, HP_MIXED = 0, 1
+HP_REAL, HP_COMPLEX = 0, 1
+HP_EULER, HP_MIDPOINT, HP_RK2, HP_RK4 = 0, 1, 2, 3
+HP_DEVICE, HP_HOST = 0, 1
+METHODS = {'euler': HP_EULER, 'midpoint': HP_MIDPOINT, 'rk2': HP_RK2, 'rk4': HP_RK4}
+
+EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set_stream',
+           'hp_last_error', 'hp_plan_set_model', 'hp_wigner_d', 'hp_quad_weights',
+           'hp_fftSO3R_forward', 'hp_fftSO3R_backward', 'hp_pendulum_propagate',
+           'hp_pendulum_derivative', 'hp_fftSO3_prod', 'hp_state_create', 'hp_state_destroy',
+           'hp_state_load', 'hp_state_store', 'hp_state_step', 'hp_state_density',
+           'hp_state_mass']
+
+
+class HPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f'hp error {code}: {msg}')
+        self.code = code
+
+
+class hp_model(ctypes.Structure):
+    _fields_ = [('L', ctypes.c_double), ('b', ctypes.c_double * 3), ('G', ctypes.c_double * 9),
+                ('gyro', ctypes.c_double * 3)]
+
+
+class hp_plan_info_t(ctypes.Structure):
+    _fields_ = [('B', ctypes.c_int), ('lmax', ctypes.c_int), ('Bx', ctypes.c_int), ('N', ctypes.c_int),
+                ('ndim', ctypes.c_int), ('precision', ctypes.c_int), ('symmetry', ctypes.c_int),
+                ('nx', ctypes.c_longlong), ('nrows', ctypes.c_longlong), ('n_full', ctypes.c_longlong),
+                ('n_grid', ctypes.c_longlong), ('state_bytes', ctypes.c_longlong)]
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f'{_LIB_PATH} is missing: build it with `python build.py` '
+                          '(the CUDA library is the only implementation; there is no fallback)')
+    lib = ctypes.CDLL(_LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    sig = {
+        'hp_plan_create': [ctypes.POINTER(vp), ip, ip, ip, ip, ip],
+        'hp_plan_destroy': [vp], 'hp_plan_get_info': [vp, ctypes.POINTER(hp_plan_info_t)],
+        'hp_plan_set_stream': [vp, vp], 'hp_plan_set_model': [vp, ctypes.POINTER(hp_model), vp, ip],
+        'hp_wigner_d': [vp, vp, ip], 'hp_quad_weights': [vp, vp, ip],
+        'hp_fftSO3R_forward': [vp, vp, vp, ip], 'hp_fftSO3R_backward': [vp, vp, vp, ip],
+        'hp_pendulum_propagate': [vp, vp, vp, dp, ip, ip], 'hp_pendulum_derivative': [vp, vp, vp, ip],
+        'hp_fftSO3_prod': [vp, vp, vp, vp, ip, ip],
+        'hp_state_create': [vp, ctypes.POINTER(vp)], 'hp_state_destroy': [vp],
+        'hp_state_load': [vp, vp, ip], 'hp_state_store': [vp, vp, ip],
+        'hp_state_step': [vp, dp, ip, ip], 'hp_state_density': [vp, vp], 'hp_state_mass': [vp, ctypes.POINTER(dp)],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.hp_last_error.restype = ctypes.c_char_p
+    lib.hp_last_error.argtypes = []
+    return lib
+
+
+_lib = _load()
+
+
+def _check(code: int):
+    if code != HP_OK:
+        raise HPError(code, _lib.hp_last_error().decode())
+
+
+def _ptr(a, dtype):
+    """(pointer, mem) of a numpy array or torch CUDA tensor with the required dtype."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != dtype:
+            raise TypeError(f'expected {dtype}, got {a.dtype}')
+        if not (a.flags['F_CONTIGUOUS'] or a.flags['C_CONTIGUOUS']):
+            raise ValueError('array must be contiguous')
+        return a.ctypes.data, HP_HOST
+    try:
+        import torch
+    except ImportError as e:  # pragma: no cover
+        raise TypeError('expected a numpy array') from e
+    if isinstance(a, torch.Tensor):
+        tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.complex128): torch.complex128,
+               np.dtype(np.float32): torch.float32}[np.dtype(dtype)]
+        if a.dtype != tdt or not a.is_contiguous():
+            raise TypeError(f'expected a contiguous {tdt} tensor')
+        return a.data_ptr(), (HP_DEVICE if a.is_cuda else HP_HOST)
+    raise TypeError(f'unsupported array type {type(a)}')
+
+
+# ------------------------------------------------------------------- plan ----
+class Plan:
+    """Tables and workspace for one (B, Bx, ndim, precision, symmetry)."""
+
+    def __init__(self, B: int, Bx: int, ndim: int, precision: int = HP_FP64, symmetry: int = HP_REAL):
+        h = ctypes.c_void_p()
+        _check(_lib.hp_plan_create(ctypes.byref(h), B, Bx, ndim, precision, symmetry))
+        self._h = h
+        self.B, self.Bx, self.ndim, self.precision, self.symmetry = B, Bx, ndim, precision, symmetry
+        info = hp_plan_info_t()
+        _check(_lib.hp_plan_get_info(h, ctypes.byref(info)))
+        self.info = info
+        self.lmax, self.N, self.nx, self.nrows = B - 1, 2 * Bx, info.nx, info.nrows
+        self.model = None
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h is not None and _lib is not None:
+            _lib.hp_plan_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # shapes (MATLAB order)
+    @property
+    def F_shape(self):
+        return (2 * self.lmax + 1, 2 * self.lmax + 1, self.lmax + 1) + (self.N,) * self.ndim
+
+    @property
+    def f_shape(self):
+        return (2 * self.B,) * 3 + (self.N,) * self.ndim
+
+    def set_stream(self, stream_ptr: int):
+        _check(_lib.hp_plan_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def set_model(self, L: float, b, G, MR, gyro=(0.0, 0.0, 0.0)):
+        m = hp_model()
+        m.L = float(L)
+        bb = list(np.asarray(b, float).ravel()) + [0.0] * 3
+        for i in range(3):
+            m.b[i] = bb[i]
+        Gm = np.zeros((3, 3))
+        Ga = np.asarray(G, float)
+        Gm[:Ga.shape[0], :Ga.shape[1]] = Ga
+        for i in range(9):
+            m.G[i] = Gm.ravel()[i]
+        for i in range(3):
+            m.gyro[i] = float(gyro[i])
+        MRc = _as_matlab(MR, np.complex128)
+        p, mem = _ptr(MRc, np.complex128)
+        _check(_lib.hp_plan_set_model(self._h, ctypes.byref(m), ctypes.c_void_p(p), mem))
+        self.model = dict(L=float(L), b=np.array(bb[:3]), G=Gm, gyro=tuple(gyro))
+        self._MR_keep = MRc
+
+    def wigner_d(self) -> np.ndarray:
+        d = np.zeros((2 * self.lmax + 1, 2 * self.lmax + 1, self.lmax + 1, 2 * self.B), order='F')
+        _check(_lib.hp_wigner_d(self._h, ctypes.c_void_p(d.ctypes.data), HP_HOST))
+        return d
+
+    def quad_weights(self) -> np.ndarray:
+        w = np.zeros(2 * self.B)
+        _check(_lib.hp_quad_weights(self._h, ctypes.c_void_p(w.ctypes.data), HP_HOST))
+        return w
+
+    # transforms -----------------------------------------------------------
+    def forward(self, f, out=None):
+        cplx = self.symmetry == HP_COMPLEX
+        fdt = np.complex128 if cplx else np.float64
+        f = _as_matlab(f, fdt)
+        if out is None:
+            out = _empty_like_mem(f, self.F_shape, np.complex128)
+        pi, mi = _ptr(f, fdt)
+        po, mo = _ptr(out, np.complex128)
+        if mi != mo:
+            raise ValueError('input and output must live in the same memory space')
+        _check(_lib.hp_fftSO3R_forward(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), mi))
+        return out
+
+    def backward(self, F, out=None):
+        cplx = self.symmetry == HP_COMPLEX
+        fdt = np.complex128 if cplx else np.float64
+        F = _as_matlab(F, np.complex128)
+        if out is None:
+            out = _empty_like_mem(F, self.f_shape, fdt)
+        pi, mi = _ptr(F, np.complex128)
+        po, mo = _ptr(out, fdt)
+        if mi != mo:
+            raise ValueError('input and output must live in the same memory space')
+        _check(_lib.hp_fftSO3R_backward(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), mi))
+        return out
+
+    def propagate(self, F, dt: float, method: str = 'euler', out=None):
+        F = _as_matlab(F, np.complex128)
+        if out is None:
+            out = _empty_like_mem(F, self.F_shape, np.complex128)
+        pi, mi = _ptr(F, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        _check(_lib.hp_pendulum_propagate(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), float(dt),
+                                          METHODS[method.lower()], mi))
+        return out
+
+    def derivative(self, F, out=None):
+        F = _as_matlab(F, np.complex128)
+        if out is None:
+            out = _empty_like_mem(F, self.F_shape, np.complex128)
+        pi, mi = _ptr(F, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        _check(_lib.hp_pendulum_derivative(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), mi))
+        return out
+
+    def prod(self, F, G, out=None):
+        F = _as_matlab(F, np.complex128)
+        G = _as_matlab(G, np.complex128)
+        batch = int(np.prod(F.shape[3:])) if F.ndim > 3 else 1
+        if out is None:
+            out = _empty_like_mem(F, F.shape, np.complex128)
+        pf, mf = _ptr(F, np.complex128)
+        pg, _ = _ptr(G, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        _check(_lib.hp_fftSO3_prod(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(pg), ctypes.c_void_p(po),
+                                   batch, mf))
+        return out
+
+
+class State:
+    """Coefficients resident on the device across steps."""
+
+    def __init__(self, plan: Plan):
+        h = ctypes.c_void_p()
+        _check(_lib.hp_state_create(plan.handle, ctypes.byref(h)))
+        self._h, self.plan = h, plan
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h is not None and _lib is not None:
+            _lib.hp_state_destroy(h)
+            self._h = None
+
+    def load(self, F):
+        F = _as_matlab(F, np.complex128)
+        p, m = _ptr(F, np.complex128)
+        _check(_lib.hp_state_load(self._h, ctypes.c_void_p(p), m))
+
+    def store(self, out=None):
+        if out is None:
+            out = np.zeros(self.plan.F_shape, np.complex128, order='F')
+        p, m = _ptr(out, np.complex128)
+        _check(_lib.hp_state_store(self._h, ctypes.c_void_p(p), m))
+        return out
+
+    def step(self, dt: float, method: str = 'euler', nsteps: int = 1):
+        _check(_lib.hp_state_step(self._h, float(dt), METHODS[method.lower()], int(nsteps)))
+
+    def density_into(self, dev_ptr: int):
+        _check(_lib.hp_state_density(self._h, ctypes.c_void_p(dev_ptr)))
+
+    def mass(self) -> float:
+        v = ctypes.c_double()
+        _check(_lib.hp_state_mass(self._h, ctypes.byref(v)))
+        return v.value
+
+
+# ---------------------------------------------------------------- helpers ----
+def _as_matlab(a, dtype):
+    """Numpy arrays are taken in MATLAB (Fortran) order; torch tensors as given
+    (their memory must already be in the MATLAB column-major order)."""
+    if isinstance(a, np.ndarray):
+        return np.asfortranarray(a, dtype=dtype)
+    return a
+
+
+def _empty_like_mem(ref, shape, dtype):
+    if isinstance(ref, np.ndarray):
+        return np.zeros(shape, dtype=dtype, order='F')
+    import torch
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.complex128): torch.complex128}[np.dtype(dtype)]
+    return torch.zeros(int(np.prod(shape)), dtype=tdt, device=ref.device)
+
+
+@lru_cache(maxsize=32)
+def get_plan(B: int, Bx: int, ndim: int, precision: int = HP_FP64, symmetry: int = HP_REAL) -> Plan:
+    return Plan(B, Bx, ndim, precision, symmetry)
+
+
+# ------------------------------------------------- reference-shaped API ----
+def getu(lmax: int) -> np.ndarray:
+    """u^l_i of getu.m:132-163 (complex harmonics): F^l[E_i f] = F^l[f] (u^l_i)^T."""
+    D = 2 * lmax + 1
+    u = np.zeros((D, D, lmax + 1, 3), np.complex128)
+    for l in range(lmax + 1):
+        for n in range(-l, l + 1):
+            if n > -l:
+                a = math.sqrt((l + n) * (l - n + 1))
+                u[n + lmax - 1, n + lmax, l, 0] = -0.5j * a
+                u[n + lmax - 1, n + lmax, l, 1] = 0.5 * a
+            if n < l:
+                a = math.sqrt((l - n) * (l + n + 1))
+                u[n + lmax + 1, n + lmax, l, 0] = -0.5j * a
+                u[n + lmax + 1, n + lmax, l, 1] = -0.5 * a
+        for m in range(-l, l + 1):
+            u[m + lmax, m + lmax, l, 2] = -1j * m
+    return u
+
+
+def _grid(Bx: int, L: float, ndim: int) -> np.ndarray:
+    N = 2 * Bx
+    g = -L / 2 + L / N * np.arange(N)
+    return np.stack(np.meshgrid(*([g] * ndim), indexing='ij'), 0)
+
+
+def _check_X(X, Bx: int, L: float, ndim: int):
+    """The MEX receives X = fftn(x) (pendulum.m:141-143); the library rebuilds x
+    from L, so X must be that table."""
+    x = _grid(Bx, L, ndim)
+    X = np.asarray(X)
+    for i in range(ndim):
+        ref = np.fft.fftn(x[i])
+        if not np.allclose(X[..., i], ref, rtol=1e-9, atol=1e-9 * np.abs(ref).max()):
+            raise HPError(HP_ERR_UNSUPPORTED, 'X is not fftn of the uniform grid over [-L/2, L/2)')
+
+
+def _fit_gyro(OJO, Bx: int, L: float):
+    """Coefficients (g1, g2, g3) with ifftn(OJO_i) = (g1 x2 x3, g2 x1 x3, g3 x1 x2),
+    the form of J^-1(-x cross Jx) for a diagonal J (pendulum.m:145-158)."""
+    x = _grid(Bx, L, 3)
+    pairs = [(1, 2), (0, 2), (0, 1)]
+    g = []
+    for i in range(3):
+        ojo = np.real(np.fft.ifftn(np.asarray(OJO)[..., i]))
+        basis = x[pairs[i][0]] * x[pairs[i][1]]
+        c = float(np.sum(ojo * basis) / np.sum(basis * basis))
+        resid = np.abs(ojo - c * basis).max()
+        if resid > 1e-8 * max(1.0, np.abs(ojo).max()):
+            raise HPError(HP_ERR_UNSUPPORTED, 'OJO is not of the diagonal-J form (g1 x2 x3, g2 x1 x3, g3 x1 x2)')
+        g.append(c)
+    return tuple(g)
+
+
+def _model_plan(F, X, OJO, MR, b, G, L, precision):
+    F = np.asarray(F)
+    lmax = F.shape[2] - 1
+    B = lmax + 1
+    ndim = F.ndim - 3
+    Bx = F.shape[3] // 2
+    _check_X(X, Bx, L, ndim)
+    gyro = _fit_gyro(OJO, Bx, L) if ndim == 3 else (0.0, 0.0, 0.0)
+    plan = get_plan(B, Bx, ndim, precision, HP_REAL)
+    plan.set_model(L, b, G, MR, gyro)
+    return plan
+
+
+def pendulum_propagate(F, X, OJO, MR, bt, G, dt, L, u, CG, method='euler'):
+    """Drop-in for the MEX pendulum_propagate(F,X,OJO,MR,bt,G,dt,L,u,CG,method)
+    (propagation/mex/sources/pendulum_propagate/kernel.cu:9-519), FP64.
+    u and CG are accepted for signature compatibility; the library uses its own
+    device tables (getu.m / clebsch_gordan.m restated on the GPU)."""
+    plan = _model_plan(F, X, OJO, MR, bt, G, L, HP_FP64)
+    return plan.propagate(F, dt, method)
+
+
+def pendulum_propagate32(F, X, OJO, MR, bt, G, dt, L, u, CG, method='euler'):
+    """Mixed-precision twin of pendulum_propagate (FP32 operators, FP64 accumulation)."""
+    plan = _model_plan(F, X, OJO, MR, bt, G, L, HP_MIXED)
+    return plan.propagate(F, dt, method)
+
+
+def pendulum_propagate_reduced(F, X, MR, bt, G, dt, L, u, CG, method='euler'):
+    """Drop-in for pendulum_propagate_reduced(F,X,MR,bt,G,dt,L,u,CG,method)
+    (propagation/mex/sources/pendulum_propagate_reduced/kernel.cu:9-262)."""
+    plan = _model_plan(F, X, None, MR, bt, G, L, HP_FP64)
+    return plan.propagate(F, dt, method)
+
+
+def pendulum_propagate_reduced32(F, X, MR, bt, G, dt, L, u, CG, method='euler'):
+    plan = _model_plan(F, X, None, MR, bt, G, L, HP_MIXED)
+    return plan.propagate(F, dt, method)
+
+
+def fftSO3R_mex(direction: str, A, d=None, w=None, precision: int = HP_FP64):
+    """Drop-in for fftSO3R_mex('forward', f, d, w) / fftSO3R_mex('backward', F, d)
+    (propagation/mex/sources/fftSO3R/kernel.cu:5-392).  d and w are accepted for
+    signature compatibility (the plan builds them on the device)."""
+    A = np.asarray(A)
+    if direction == 'forward':
+        B, Bx, ndim = A.shape[0] // 2, A.shape[3] // 2, A.ndim - 3
+        return get_plan(B, Bx, ndim, precision, HP_REAL).forward(A)
+    if direction == 'backward':
+        B, Bx, ndim = A.shape[2], A.shape[3] // 2, A.ndim - 3
+        return get_plan(B, Bx, ndim, precision, HP_REAL).backward(A)
+    raise ValueError("direction must be 'forward' or 'backward'")
+
+
+def fftSO3R(f, precision: int = HP_FP64):
+    """F = fftSO3R(f) for grid samples f (fftSO3R.m:89-106); complex f gives a complex plan."""
+    f = np.asarray(f)
+    B, Bx, ndim = f.shape[0] // 2, f.shape[3] // 2, f.ndim - 3
+    sym = HP_COMPLEX if np.iscomplexobj(f) else HP_REAL
+    return get_plan(B, Bx, ndim, precision, sym).forward(f)
+
+
+def ifftSO3R(F, isreal: bool = True, precision: int = HP_FP64):
+    """f = ifftSO3R(F) (ifftSO3R.m:16-37); isreal=True returns the real density
+    (the 'symmetric' inverse of pendulum.m:303), False the complex samples."""
+    F = np.asarray(F)
+    B, Bx, ndim = F.shape[2], F.shape[3] // 2, F.ndim - 3
+    return get_plan(B, Bx, ndim, precision, HP_REAL if isreal else HP_COMPLEX).backward(F)
+
+
+def fftSO3_prod(F, G):
+    """FG of fftSO3_prod.m:247-264 from coefficient arrays F, G of shape
+    (2lmax+1, 2lmax+1, lmax+1[, batch...]).  A batch of 1 uses any omega plan
+    of the same B; the grid product fg is not returned (no function handles)."""
+    F = np.asarray(F)
+    B = F.shape[2]
+    return get_plan(B, 2, 2, HP_FP64, HP_REAL).prod(F, G)

@@ -1,0 +1,434 @@
+// C ABI (include/hp.h): plans, host/device staging, integrators, state API.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "plan.hpp"
+
+using namespace hp;
+
+static thread_local std::string g_err;
+void hp_set_error(const char* msg) { g_err = msg ? msg : ""; }
+extern "C" const char* hp_last_error(void) { return g_err.c_str(); }
+
+#define HP_CHECK(expr)              \
+  do {                              \
+    int _s = (expr);                \
+    if (_s != HP_OK) return _s;     \
+  } while (0)
+
+void* hp_plan::ws_get(const char* name, size_t bytes, int* status) {
+  for (auto& kv : ws) {
+    if (kv.first == name) {
+      if (kv.second.bytes >= bytes) return kv.second.p;
+      cudaFree(kv.second.p);
+      kv.second = Buf{};
+      void* q = nullptr;
+      if (cudaMalloc(&q, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        hp_set_error("device allocation failed");
+        *status = HP_ERR_ALLOC;
+        return nullptr;
+      }
+      kv.second = Buf{q, bytes};
+      return q;
+    }
+  }
+  void* q = nullptr;
+  if (cudaMalloc(&q, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    hp_set_error("device allocation failed");
+    *status = HP_ERR_ALLOC;
+    return nullptr;
+  }
+  ws.push_back({name, Buf{q, bytes}});
+  return q;
+}
+
+static bool valid_N(int N) {
+  return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 32;
+}
+static bool valid_B(int B) {
+  switch (B) {
+    case 2: case 3: case 4: case 5: case 6: case 8: case 10: case 12: case 15: case 16: case 20: case 32:
+      return true;
+    default:
+      return false;
+  }
+}
+
+extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precision, int symmetry) {
+  if (!out) { hp_set_error("plan pointer is null"); return HP_ERR_INVALID; }
+  *out = nullptr;
+  if (!valid_B(B)) { hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,32)"); return HP_ERR_INVALID; }
+  if (!valid_N(2 * Bx)) { hp_set_error("2*Bx must be one of 4,6,8,12,16,20,24,32"); return HP_ERR_INVALID; }
+  if (ndim != 2 && ndim != 3) { hp_set_error("ndim must be 2 or 3"); return HP_ERR_INVALID; }
+  if (precision != HP_FP64 && precision != HP_MIXED) { hp_set_error("bad precision"); return HP_ERR_INVALID; }
+  if (symmetry != HP_REAL && symmetry != HP_COMPLEX) { hp_set_error("bad symmetry"); return HP_ERR_INVALID; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    hp_set_error("no CUDA device");
+    return HP_ERR_CUDA;
+  }
+  hp_plan* p = new hp_plan();
+  p->B = B; p->lmax = B - 1; p->Bx = Bx; p->N = 2 * Bx; p->ndim = ndim;
+  p->precision = precision; p->symmetry = symmetry;
+  p->D = 2 * p->lmax + 1;
+  p->m_lo = symmetry == HP_REAL ? 0 : -p->lmax;
+  p->nm = p->lmax - p->m_lo + 1;
+  p->nx = 1;
+  for (int a = 0; a < ndim; ++a) p->nx *= p->N;
+  int st = hp_tables_build(p);
+  if (st) { hp_plan_destroy(p); return st; }
+  *out = p;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_destroy(hp_plan* p) {
+  if (!p) return HP_OK;
+  cudaFree(p->rows); cudaFree(p->seg); cudaFree(p->wig64); cudaFree(p->wig32); cudaFree(p->wfull);
+  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_row); cudaFree(p->tap_w);
+  for (auto& kv : p->ws) cudaFree(kv.second.p);
+  delete p;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_get_info(const hp_plan* p, hp_plan_info_t* info) {
+  if (!p || !info) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  info->B = p->B; info->lmax = p->lmax; info->Bx = p->Bx; info->N = p->N; info->ndim = p->ndim;
+  info->precision = p->precision; info->symmetry = p->symmetry;
+  info->nx = p->nx; info->nrows = p->nrows; info->n_full = p->n_full(); info->n_grid = p->n_grid();
+  info->state_bytes = 16LL * p->nrows * p->nx;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_set_stream(hp_plan* p, void* s) {
+  if (!p) { hp_set_error("null plan"); return HP_ERR_INVALID; }
+  p->stream = (cudaStream_t)s;
+  return HP_OK;
+}
+
+// ------------------------------------------------------------ staging ----
+// Returns a device pointer holding `bytes` of `src` (copied when on the host).
+static const void* stage_in(hp_plan* p, const char* name, const void* src, size_t bytes, int mem, int* st) {
+  if (mem == HP_DEVICE) return src;
+  void* d = p->ws_get(name, bytes, st);
+  if (*st) return nullptr;
+  if (cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, p->stream) != cudaSuccess) {
+    hp_set_error("host to device copy failed");
+    *st = HP_ERR_CUDA;
+    return nullptr;
+  }
+  return d;
+}
+static void* stage_out(hp_plan* p, const char* name, void* dst, size_t bytes, int mem, int* st) {
+  if (mem == HP_DEVICE) return dst;
+  return p->ws_get(name, bytes, st);
+}
+static int finish_out(hp_plan* p, void* host, const void* dev, size_t bytes, int mem) {
+  if (mem == HP_DEVICE) return HP_OK;
+  HP_CUDA_TRY(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+static int check_mem(int mem) {
+  if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("mem must be HP_DEVICE or HP_HOST"); return HP_ERR_INVALID; }
+  return HP_OK;
+}
+
+// ---------------------------------------------------------------- model ----
+extern "C" int hp_plan_set_model(hp_plan* p, const hp_model* m, const double* MR, int mem) {
+  if (!p || !m || !MR) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  if (!(m->L > 0) || !std::isfinite(m->L)) { hp_set_error("L must be positive"); return HP_ERR_INVALID; }
+  const int D = p->D, lmax = p->lmax;
+  const size_t nMR = (size_t)D * D * (lmax + 1) * p->ndim;
+  std::vector<double2> h(nMR);
+  if (mem == HP_HOST) std::memcpy(h.data(), MR, sizeof(double2) * nMR);
+  else HP_CUDA_TRY(cudaMemcpy(h.data(), MR, sizeof(double2) * nMR, cudaMemcpyDeviceToHost));
+  // only the degree-1, m2 = 0 block may carry weight (gravity depends on R^T e3)
+  double big = 0.0, stray = 0.0;
+  for (int i = 0; i < p->ndim; ++i)
+    for (int l = 0; l <= lmax; ++l)
+      for (int n = -l; n <= l; ++n)
+        for (int mm = -l; mm <= l; ++mm) {
+          const double2 v = h[(mm + lmax) + (size_t)D * (n + lmax) + (size_t)D * D * l + (size_t)D * D * (lmax + 1) * i];
+          const double a = std::hypot(v.x, v.y);
+          if (!std::isfinite(a)) { hp_set_error("MR has non-finite entries"); return HP_ERR_NONFINITE; }
+          if (l == 1 && mm == 0) big = std::max(big, a);
+          else stray = std::max(stray, a);
+        }
+  if (stray > 1e-9 * std::max(big, 1e-300) && stray > 1e-300) {
+    hp_set_error("MR has components outside the degree-1, m2=0 block (alpha-dependent multiplier)");
+    return HP_ERR_UNSUPPORTED;
+  }
+  int st = HP_OK;
+  double2* dMR = (double2*)p->ws_get("model.MR", sizeof(double2) * nMR, &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaMemcpy(dMR, h.data(), sizeof(double2) * nMR, cudaMemcpyHostToDevice));
+  HP_CHECK(hp_build_gravity_taps(p, dMR));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  p->model = *m;
+  p->has_model = true;
+  return HP_OK;
+}
+
+extern "C" int hp_wigner_d(hp_plan* p, double* d, int mem) {
+  if (!p || !d) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  const size_t n = (size_t)p->D * p->D * (p->lmax + 1) * 2 * p->B;
+  HP_CUDA_TRY(cudaMemcpy(d, p->wfull, sizeof(double) * n, mem == HP_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+  return HP_OK;
+}
+
+extern "C" int hp_quad_weights(hp_plan* p, double* w, int mem) {
+  if (!p || !w) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  HP_CUDA_TRY(cudaMemcpy(w, p->qw, sizeof(double) * 2 * p->B, mem == HP_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice));
+  return HP_OK;
+}
+
+// ----------------------------------------------------- grid conversions ----
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+
+// ----------------------------------------------------------- transforms ----
+extern "C" int hp_fftSO3R_forward(hp_plan* p, const double* f, double* F, int mem) {
+  if (!p || !f || !F) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  int st = HP_OK;
+  const bool cplx = p->symmetry == HP_COMPLEX;
+  const long long ng = p->n_grid() * (cplx ? 2 : 1);
+  const double* df = (const double*)stage_in(p, "api.fin", f, sizeof(double) * ng, mem, &st);
+  if (st) return st;
+  const void* src = df;
+  if (p->precision == HP_MIXED) {
+    float* t = (float*)p->ws_get("api.f32", sizeof(float) * ng, &st);
+    if (st) return st;
+    k_d2f<<<(unsigned)((ng + 255) / 256), 256, 0, p->stream>>>(df, t, ng);
+    HP_CUDA_TRY(cudaGetLastError());
+    src = t;
+  }
+  double2* Fi = (double2*)p->ws_get("api.Fint", 16 * (size_t)p->nrows * p->nx, &st);
+  if (st) return st;
+  HP_CHECK(hp_forward_internal(p, src, cplx, Fi, p->stream));
+  double2* dF = (double2*)stage_out(p, "api.Fout", F, 16 * (size_t)p->n_full(), mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_internal_to_full(p, Fi, dF, p->stream));
+  HP_CHECK(finish_out(p, F, dF, 16 * (size_t)p->n_full(), mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_fftSO3R_backward(hp_plan* p, const double* F, double* f, int mem) {
+  if (!p || !F || !f) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  int st = HP_OK;
+  const bool cplx = p->symmetry == HP_COMPLEX;
+  const long long ng = p->n_grid() * (cplx ? 2 : 1);
+  const double2* dF = (const double2*)stage_in(p, "api.Fin", F, 16 * (size_t)p->n_full(), mem, &st);
+  if (st) return st;
+  double2* Fi = (double2*)p->ws_get("api.Fint", 16 * (size_t)p->nrows * p->nx, &st);
+  if (st) return st;
+  HP_CHECK(hp_full_to_internal(p, dF, Fi, p->stream));
+  double* df = (double*)stage_out(p, "api.fout", f, sizeof(double) * ng, mem, &st);
+  if (st) return st;
+  if (p->precision == HP_MIXED) {
+    float* t = (float*)p->ws_get("api.f32", sizeof(float) * ng, &st);
+    if (st) return st;
+    HP_CHECK(hp_backward_internal(p, Fi, t, cplx, p->stream));
+    k_f2d<<<(unsigned)((ng + 255) / 256), 256, 0, p->stream>>>(t, df, ng);
+    HP_CUDA_TRY(cudaGetLastError());
+  } else {
+    HP_CHECK(hp_backward_internal(p, Fi, df, cplx, p->stream));
+  }
+  HP_CHECK(finish_out(p, f, df, sizeof(double) * ng, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+// ----------------------------------------------------------- integrators ----
+// One step of `method` on internal-layout buffers; the result lands in *F
+// (buffers are swapped, never aliased inside one derivative evaluation).
+static int integrate_internal(hp_plan* p, double2** F, double2** F2, double2** F3, double2* acc, double dt,
+                              int method) {
+  cudaStream_t s = p->stream;
+  const size_t bytes = 16 * (size_t)p->nrows * p->nx;
+  switch (method) {
+    case HP_EULER:
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, nullptr, 0.0, s));
+      std::swap(*F, *F2);
+      return HP_OK;
+    case HP_MIDPOINT:
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F2, *F, dt, *F3, nullptr, 0.0, s));
+      std::swap(*F, *F3);
+      return HP_OK;
+    case HP_RK2:
+      HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, acc, dt / 2, s));
+      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 2, *F3, nullptr, 0.0, s));
+      std::swap(*F, *F3);
+      return HP_OK;
+    case HP_RK4:
+      HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, acc, dt / 6, s));
+      HP_CHECK(hp_derivative_eval(p, *F2, *F, dt / 2, *F3, acc, dt / 3, s));
+      HP_CHECK(hp_derivative_eval(p, *F3, *F, dt, *F2, acc, dt / 3, s));
+      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 6, *F3, nullptr, 0.0, s));
+      std::swap(*F, *F3);
+      return HP_OK;
+    default:
+      hp_set_error("method must be HP_EULER, HP_MIDPOINT, HP_RK2 or HP_RK4");
+      return HP_ERR_INVALID;
+  }
+}
+
+extern "C" int hp_pendulum_propagate(hp_plan* p, const double* Fold, double* Fnew, double dt, int method,
+                                     int mem) {
+  if (!p || !Fold || !Fnew) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
+  if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
+  int st = HP_OK;
+  const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
+  const double2* dF = (const double2*)stage_in(p, "api.Fin", Fold, fb, mem, &st);
+  if (st) return st;
+  double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
+  double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
+  double2* b2 = (method == HP_EULER) ? nullptr : (double2*)p->ws_get("api.S2", ib, &st); if (st) return st;
+  double2* ac = (method == HP_RK2 || method == HP_RK4) ? (double2*)p->ws_get("api.S3", ib, &st) : nullptr;
+  if (st) return st;
+  HP_CHECK(hp_full_to_internal(p, dF, b0, p->stream));
+  double2 *F = b0, *F2 = b1, *F3 = b2;
+  HP_CHECK(integrate_internal(p, &F, &F2, &F3, ac, dt, method));
+  double2* dOut = (double2*)stage_out(p, "api.Fout", Fnew, fb, mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_internal_to_full(p, F, dOut, p->stream));
+  HP_CHECK(finish_out(p, Fnew, dOut, fb, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_pendulum_derivative(hp_plan* p, const double* F, double* dF, int mem) {
+  if (!p || !F || !dF) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  int st = HP_OK;
+  const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
+  const double2* dIn = (const double2*)stage_in(p, "api.Fin", F, fb, mem, &st);
+  if (st) return st;
+  double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
+  double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
+  HP_CHECK(hp_full_to_internal(p, dIn, b0, p->stream));
+  HP_CHECK(hp_derivative_eval(p, b0, nullptr, 1.0, b1, nullptr, 0.0, p->stream));
+  double2* dOut = (double2*)stage_out(p, "api.Fout", dF, fb, mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_internal_to_full(p, b1, dOut, p->stream));
+  HP_CHECK(finish_out(p, dF, dOut, fb, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_fftSO3_prod(hp_plan* p, const double* F, const double* G, double* FG, int batch, int mem) {
+  if (!p || !F || !G || !FG || batch < 1) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  int st = HP_OK;
+  const size_t nb = 16 * (size_t)p->D * p->D * p->B * batch;
+  const double2* dFa = (const double2*)stage_in(p, "prod.F", F, nb, mem, &st); if (st) return st;
+  const double2* dGa = (const double2*)stage_in(p, "prod.G", G, nb, mem, &st); if (st) return st;
+  double2* dO = (double2*)stage_out(p, "prod.FG", FG, nb, mem, &st); if (st) return st;
+  HP_CHECK(hp_prod_launch(p, dFa, dGa, dO, batch, p->stream));
+  HP_CHECK(finish_out(p, FG, dO, nb, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+// ---------------------------------------------------------------- state ----
+extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
+  if (!p || !out) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  *out = nullptr;
+  hp_state* s = new hp_state();
+  s->plan = p;
+  const size_t ib = 16 * (size_t)p->nrows * p->nx;
+  double2** bufs[4] = {&s->F, &s->F2, &s->F3, &s->acc};
+  for (auto b : bufs) {
+    if (cudaMalloc(b, ib) != cudaSuccess) {
+      cudaGetLastError();
+      hp_state_destroy(s);
+      hp_set_error("device allocation failed");
+      return HP_ERR_ALLOC;
+    }
+  }
+  HP_CUDA_TRY(cudaMemset(s->F, 0, ib));
+  *out = s;
+  return HP_OK;
+}
+
+extern "C" int hp_state_destroy(hp_state* s) {
+  if (!s) return HP_OK;
+  cudaFree(s->F); cudaFree(s->F2); cudaFree(s->F3); cudaFree(s->acc);
+  delete s;
+  return HP_OK;
+}
+
+extern "C" int hp_state_load(hp_state* s, const double* F, int mem) {
+  if (!s || !F) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  hp_plan* p = s->plan;
+  int st = HP_OK;
+  const double2* d = (const double2*)stage_in(p, "api.Fin", F, 16 * (size_t)p->n_full(), mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_full_to_internal(p, d, s->F, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_state_store(hp_state* s, double* F, int mem) {
+  if (!s || !F) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  hp_plan* p = s->plan;
+  int st = HP_OK;
+  const size_t fb = 16 * (size_t)p->n_full();
+  double2* d = (double2*)stage_out(p, "api.Fout", F, fb, mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_internal_to_full(p, s->F, d, p->stream));
+  HP_CHECK(finish_out(p, F, d, fb, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
+  if (!s || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  hp_plan* p = s->plan;
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  for (int k = 0; k < nsteps; ++k) HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
+  return HP_OK;
+}
+
+extern "C" int hp_state_density(hp_state* s, void* f) {
+  if (!s || !f) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  hp_plan* p = s->plan;
+  return hp_backward_internal(p, s->F, f, p->symmetry == HP_COMPLEX, p->stream);
+}
+
+extern "C" int hp_state_mass(hp_state* s, double* mass) {
+  if (!s || !mass) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  hp_plan* p = s->plan;
+  // row (l=0, m=0, n=0) at omega index 0
+  const long long row = p->h_seg[(size_t)(0 - p->m_lo) * p->D + p->lmax];
+  double2 v;
+  HP_CUDA_TRY(cudaMemcpyAsync(&v, s->F + row * p->nx, sizeof(double2), cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  *mass = v.x;
+  return HP_OK;
+}

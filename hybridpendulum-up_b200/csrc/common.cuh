@@ -1,0 +1,162 @@
+// Common device/host helpers for the SO(3) x R^n Fokker-Planck kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/hp.h"
+
+#define HP_CUDA_TRY(expr)                                                     \
+  do {                                                                        \
+    cudaError_t _e = (expr);                                                  \
+    if (_e != cudaSuccess) { hp_set_error(cudaGetErrorString(_e)); return HP_ERR_CUDA; } \
+  } while (0)
+
+void hp_set_error(const char* msg);
+
+namespace hp {
+
+// ------------------------------------------------------------- complex ----
+template <typename T> struct C2T;
+template <> struct C2T<double> { using type = double2; };
+template <> struct C2T<float> { using type = float2; };
+template <typename T> using c2 = typename C2T<T>::type;
+
+__host__ __device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__host__ __device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(s * a.x, s * a.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a + b * c
+__device__ __forceinline__ double2 cfma(double2 b, double2 c, double2 a) {
+  return make_double2(fma(b.x, c.x, fma(-b.y, c.y, a.x)), fma(b.x, c.y, fma(b.y, c.x, a.y)));
+}
+__device__ __forceinline__ float2 cfma(float2 b, float2 c, float2 a) {
+  return make_float2(fmaf(b.x, c.x, fmaf(-b.y, c.y, a.x)), fmaf(b.x, c.y, fmaf(b.y, c.x, a.y)));
+}
+// i * a
+template <typename C> __device__ __forceinline__ C cI(C a) { C r; r.x = -a.y; r.y = a.x; return r; }
+template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+
+template <typename Cout, typename Cin> __device__ __forceinline__ Cout cvt(Cin a);
+template <> __device__ __forceinline__ double2 cvt<double2, double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 cvt<float2, float2>(float2 a) { return a; }
+template <> __device__ __forceinline__ float2 cvt<float2, double2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <> __device__ __forceinline__ double2 cvt<double2, float2>(float2 a) { return make_double2(a.x, a.y); }
+
+template <typename C> __device__ __forceinline__ C czero() { C r; r.x = 0; r.y = 0; return r; }
+
+// ------------------------------------------------------------ twiddles ----
+// W[k] = exp(-2 pi i k / 960); every transform length used here divides 960.
+// Each translation unit holds its own copy (no relocatable device code) and
+// fills it once per device with tw_init() before its first launch.
+constexpr int kTwN = 960;
+static __constant__ double2 c_tw64[kTwN];
+static __constant__ float2 c_tw32[kTwN];
+
+int tw_fill_host(double2* t64, float2* t32);  // defined in tables.cu
+
+static inline int tw_init() {
+  static unsigned long long done_mask = 0ULL;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 4;
+  if (dev < 64 && (done_mask >> dev) & 1ULL) return 0;
+  static double2 t64[kTwN];
+  static float2 t32[kTwN];
+  tw_fill_host(t64, t32);
+  if (cudaMemcpyToSymbol(c_tw64, t64, sizeof(t64)) != cudaSuccess) return 4;
+  if (cudaMemcpyToSymbol(c_tw32, t32, sizeof(t32)) != cudaSuccess) return 4;
+  if (dev < 64) done_mask |= 1ULL << dev;
+  return 0;
+}
+
+template <typename C> __device__ __forceinline__ C tw_load(int idx);
+template <> __device__ __forceinline__ double2 tw_load<double2>(int idx) { return c_tw64[idx]; }
+template <> __device__ __forceinline__ float2 tw_load<float2>(int idx) { return c_tw32[idx]; }
+
+// exp(-+ 2 pi i e / M) (INV selects +)
+template <typename C, bool INV>
+__device__ __forceinline__ C twiddle(int e, int M) {
+  C w = tw_load<C>(((e % M) * (kTwN / M)) % kTwN);
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+// ------------------------------------------------- register-resident FFT ----
+// Small DFT of radix R in registers (out-of-place on v).
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void dft_small(C (&v)[R]) {
+  if constexpr (R == 2) {
+    C a = v[0], b = v[1];
+    v[0] = a + b; v[1] = a - b;
+  } else if constexpr (R == 4) {
+    C t0 = v[0] + v[2], t1 = v[0] - v[2], t2 = v[1] + v[3], t3 = v[1] - v[3];
+    // forward: multiply t3 by -i ; inverse: by +i
+    C t3r;
+    if (INV) { t3r.x = -t3.y; t3r.y = t3.x; } else { t3r.x = t3.y; t3r.y = -t3.x; }
+    v[0] = t0 + t2; v[2] = t0 - t2; v[1] = t1 + t3r; v[3] = t1 - t3r;
+  } else {
+    C o[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      C acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) acc = cfma(v[r], twiddle<C, INV>(r * q, R), acc);
+      o[q] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = o[q];
+  }
+}
+
+template <int N, int Ns>
+struct FftRadix {
+  static constexpr int rem = N / Ns;
+  static constexpr int value = (rem % 4 == 0) ? 4 : (rem % 2 == 0 ? 2 : (rem % 3 == 0 ? 3 : (rem % 5 == 0 ? 5 : rem)));
+};
+
+// Stockham self-sorting FFT stages: unnormalised, X[k] = sum_j x[j] exp(-+2 pi i jk/N).
+template <int N, int Ns, bool INV, typename C>
+__device__ __forceinline__ void fft_stages(C (&x)[N]) {
+  if constexpr (Ns < N) {
+    constexpr int R = FftRadix<N, Ns>::value;
+    C y[N];
+#pragma unroll
+    for (int j = 0; j < N / R; ++j) {
+      const int k = j % Ns;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = x[j + r * (N / R)];
+#pragma unroll
+      for (int r = 1; r < R; ++r)
+        if ((r * k) % (Ns * R) != 0) v[r] = cmul(v[r], twiddle<C, INV>(r * k, Ns * R));
+      dft_small<R, INV>(v);
+      const int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) y[idxD + r * Ns] = v[r];
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[i] = y[i];
+    fft_stages<N, Ns * R, INV>(x);
+  }
+}
+
+template <int N, bool INV, typename C>
+__device__ __forceinline__ void fft(C (&x)[N]) { fft_stages<N, 1, INV>(x); }
+
+// Fourier index k (FFT order) -> signed wavenumber with the Nyquist bin zeroed
+// (the 2 pi i [0:Bx-1, 0, -Bx+1:-1] / L multiplier of the first derivative).
+__host__ __device__ __forceinline__ int kappa_first(int k, int N) {
+  return (k < N / 2) ? k : (k == N / 2 ? 0 : k - N);
+}
+// Signed wavenumber keeping the Nyquist bin as -N/2 (the diagonal diffusion term).
+__host__ __device__ __forceinline__ int kappa_diag(int k, int N) { return (k < N / 2) ? k : k - N; }
+
+}  // namespace hp

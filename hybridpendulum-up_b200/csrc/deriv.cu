@@ -1,0 +1,421 @@
+// Pendulum Fokker-Planck derivative and integrator update on the internal
+// coefficient layout (see plan.hpp).
+//
+// The reference forms every Omega-dependent term as an O(nx^2) circular
+// convolution with X, bX or OJO (pendulum.m:396-466).  Here the same operators
+// are applied exactly as 1-D maps along the omega axes: multiplication by the
+// grid coordinate x_i in physical space is
+//     M_i F = FFT_i( x_i . IFFT_i F )      (== (1/N) X_i (*) F along axis i),
+// so with P3 = M_3 F the derivative is
+//   dF = -(M_1F)u_1^T - (M_2F)u_2^T - (M_3F)u_3^T            Lie term   (pendulum.m:396-422)
+//        + sum_i b_i D_i M_i F                               damping    (pendulum.m:424-446)
+//        - g_1 D_1 M_2 P3 - g_2 D_2 M_1 P3 - g_3 D_3 M_1 M_2 F   gyroscopic (pendulum.m:448-466)
+//        - sum_i D_i Grav_i(F)                               gravity    (pendulum.m:470-506)
+//        + sum_ij G_ij c_ij F                                diffusion  (pendulum.m:510-523)
+// with D_i = 2 pi i kappa_i / L (Nyquist zeroed) and (g_1, g_2, g_3) the
+// coefficients of J^-1(-x cross Jx) = (g_1 x2 x3, g_2 x1 x3, g_3 x1 x2).
+//
+// Three passes (ndim = 3):
+//   k_axis3   : P3 = M_3 F            (lines along k3, one thread per line, registers only)
+//   k_local   : G  = gravity + noise  (pointwise in omega, all rows of an m group)
+//   k_plane   : 2-D (k1, k2) work of every remaining term on one k3 plane of a
+//               tile of n-consecutive rows, then out = F0 + a dF (+ acc += b dF).
+// For ndim = 2 the plane pass covers the whole omega grid and k_axis3 is skipped.
+#include <vector>
+#include "common.cuh"
+#include "plan.hpp"
+
+using namespace hp;
+
+struct DerivParams {
+  double L;
+  double b[3];
+  double G[9];
+  double gyro[3];
+};
+
+// -------------------------------------------------------- pass A: axis 3 ----
+template <int N, typename T>
+__global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __restrict__ F,
+                                               c2<T>* __restrict__ P3, T Llen) {
+  using C = c2<T>;
+  constexpr long long plane = (long long)N * N;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * plane) return;
+  const long long row = t / plane, p = t % plane;
+  const double2* src = F + row * L.nx + p;
+  C x[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) x[j] = cvt<C, double2>(__ldg(src + j * plane));
+  fft<N, true>(x);
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const T xc = (-Llen / 2 + Llen * (T)j / (T)N) / (T)N;
+    x[j] = xc * x[j];
+  }
+  fft<N, false>(x);
+  C* dst = P3 + row * L.nx + p;
+#pragma unroll
+  for (int j = 0; j < N; ++j) dst[j * plane] = x[j];
+}
+
+// ------------------------------------------------ pass B: gravity + noise ----
+// One thread per omega point, looping over the rows of one m group (taps stay
+// within the group because the gravity multiplier has m2 = 0).
+template <typename T>
+__global__ void __launch_bounds__(128) k_local(RowLayout L, const double2* __restrict__ F,
+                                               c2<T>* __restrict__ G, const int* __restrict__ tap_row,
+                                               const double2* __restrict__ tap_w, DerivParams prm) {
+  using C = c2<T>;
+  const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (w >= L.nx) return;
+  const int N = L.N, nd = L.ndim;
+  int kk[3] = {0, 0, 0};
+  long long ww = w;
+  for (int a = 0; a < nd; ++a) { kk[a] = (int)(ww % N); ww /= N; }
+  const double tp = 2.0 * M_PI / prm.L;
+  double d1[3], dd[3];
+  for (int a = 0; a < nd; ++a) {
+    d1[a] = tp * kappa_first(kk[a], N);
+    dd[a] = tp * kappa_diag(kk[a], N);
+  }
+  double noise = 0.0;
+  for (int i = 0; i < nd; ++i)
+    for (int j = 0; j < nd; ++j)
+      noise += (i == j) ? -prm.G[i * 3 + j] * dd[i] * dd[i] : -prm.G[i * 3 + j] * d1[i] * d1[j];
+  // rows of group m = blockIdx.y + m_lo
+  const int D = 2 * L.lmax + 1;
+  const int m = (int)blockIdx.y + L.m_lo;
+  const long long r0 = L.seg[(m - L.m_lo) * D + 0];
+  const long long r1 = (m + 1 <= L.lmax) ? (long long)L.seg[(m + 1 - L.m_lo) * D] : L.nrows;
+  for (long long r = r0; r < r1; ++r) {
+    const double2 f0 = F[r * L.nx + w];
+    double2 acc = make_double2(noise * f0.x, noise * f0.y);
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const int src = tap_row[r * 9 + t];
+      if (src < 0) continue;
+      // coef = -sum_i (i d1_i) W_i
+      double cx = 0.0, cy = 0.0;
+      for (int i = 0; i < nd; ++i) {
+        const double2 wv = tap_w[((long long)i * L.nrows + r) * 9 + t];
+        cx += d1[i] * wv.y;    // -(i d)(wx + i wy) = d wy - i d wx
+        cy -= d1[i] * wv.x;
+      }
+      const double2 fs = F[(long long)src * L.nx + w];
+      acc.x += cx * fs.x - cy * fs.y;
+      acc.y += cx * fs.y + cy * fs.x;
+    }
+    G[r * L.nx + w] = cvt<C, double2>(acc);
+  }
+}
+
+// --------------------------------------------------- pass C: plane pass ----
+struct PlaneTile { int m, l, n0, cnt; };
+
+template <typename T> struct PlaneCfg;
+template <> struct PlaneCfg<double> { static constexpr int C = 2; };
+template <> struct PlaneCfg<float> { static constexpr int C = 4; };
+
+__device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, int n) {
+  const int am = abs(m), an = abs(n);
+  return L.seg[(m - L.m_lo) * (2 * L.lmax + 1) + n + L.lmax] + l - (am > an ? am : an);
+}
+
+// smem planes (stride PS = N*(N+1)):
+//   [0, C+2)           F~ rows n0-1 .. n0+C     (physical after the inverse FFTs)
+//   [C+2, 2C+2)        P~ rows n0 .. n0+C-1     (ndim = 3)
+//   [2C+2, 3C+2)       A  = FFT2(Y0) + D_2 FFT2(Y2), then FFT_1
+//   [3C+2, 4C+2)       Y1' = FFT_2(Y1), then D_1 FFT_1
+template <int N, typename T, bool HAS_P3>
+__global__ void __launch_bounds__(256, 1) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
+                                                  const double2* __restrict__ Fev,
+                                                  const c2<T>* __restrict__ P3,
+                                                  const c2<T>* __restrict__ Gl,
+                                                  const double2* __restrict__ F0, double a,
+                                                  double2* __restrict__ out,
+                                                  double2* __restrict__ acc, double bacc,
+                                                  DerivParams prm) {
+  using C = c2<T>;
+  constexpr int CT = PlaneCfg<T>::C;
+  constexpr int PS = N * (N + 1);
+  constexpr int NP = HAS_P3 ? CT : 0;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  C* sF = sm;
+  C* sP = sm + (CT + 2) * PS;
+  C* sA = sm + (CT + 2 + NP) * PS;
+  C* sY = sm + (CT + 2 + NP + CT) * PS;
+
+  const PlaneTile tl = tiles[blockIdx.x];
+  const int k3 = HAS_P3 ? (int)blockIdx.y : 0;
+  const long long pbase = (long long)k3 * N * N;  // plane offset inside a row
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const T Ll = (T)prm.L;
+  const T tp = (T)(2.0 * M_PI / prm.L);
+  const T inv_n2 = (T)1 / (T)(N * N);
+
+  // ---- S1: load F rows n0-1 .. n0+cnt and P3 rows n0 .. n0+cnt-1 ----
+  const int nF = tl.cnt + 2;
+  for (int e = tid; e < nF * N * N; e += nth) {
+    const int s = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
+    const int n = tl.n0 - 1 + s;
+    C v = czero<C>();
+    if (n >= -tl.l && n <= tl.l) {
+      const long long r = row_of(L, tl.l, tl.m, n);
+      v = cvt<C, double2>(Fev[r * L.nx + pbase + q]);
+    }
+    sF[s * PS + k2 * (N + 1) + k1] = v;
+  }
+  if (HAS_P3) {
+    for (int e = tid; e < tl.cnt * N * N; e += nth) {
+      const int s = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
+      const long long r = row_of(L, tl.l, tl.m, tl.n0 + s);
+      sP[s * PS + k2 * (N + 1) + k1] = P3[r * L.nx + pbase + q];
+    }
+  }
+  __syncthreads();
+
+  // ---- S2/S3: inverse FFT along k1 (rows) then k2 (columns) of all loaded planes ----
+  const int nLoaded = nF + (HAS_P3 ? tl.cnt : 0);
+  auto plane_ptr = [&](int s) -> C* { return s < nF ? sF + s * PS : sP + (s - nF) * PS; };
+  for (int it = tid; it < nLoaded * N; it += nth) {
+    C* pl = plane_ptr(it / N);
+    const int k2 = it % N;
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = pl[k2 * (N + 1) + j];
+    fft<N, true>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) pl[k2 * (N + 1) + j] = x[j];
+  }
+  __syncthreads();
+  for (int it = tid; it < nLoaded * N; it += nth) {
+    C* pl = plane_ptr(it / N);
+    const int k1 = it % N;
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = pl[j * (N + 1) + k1];
+    fft<N, true>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) pl[j * (N + 1) + k1] = inv_n2 * x[j];
+  }
+  __syncthreads();
+
+  // ---- S4: physical-space products, forward FFT along k2 ----
+  // item (c, j1, kind): kind 0 -> A column, kind 1 -> Y1' column
+  const T d3 = HAS_P3 ? tp * (T)kappa_first(k3, N) : (T)0;
+  const T b1 = (T)prm.b[0], b2 = (T)prm.b[1], b3 = (T)prm.b[2];
+  const T g1 = (T)prm.gyro[0], g2 = (T)prm.gyro[1], g3 = (T)prm.gyro[2];
+  for (int it = tid; it < tl.cnt * N * 2; it += nth) {
+    const int kind = it / (tl.cnt * N);
+    const int c = (it / N) % tl.cnt;
+    const int j1 = it % N;
+    const T x1 = -Ll / 2 + Ll * (T)j1 / (T)N;
+    const C* f0 = sF + (c + 1) * PS;
+    const C* fm = sF + c * PS;
+    const C* fp = sF + (c + 2) * PS;
+    const C* pp = sP + c * PS;
+    const int n = tl.n0 + c, l = tl.l;
+    const T ap = sqrt((T)((l - n) * (l + n + 1))), am = sqrt((T)((l + n) * (l - n + 1)));
+    C x[N];
+    if (kind == 0) {
+      // Y0 = a+ F~+ (0.5i x1 - 0.5 x2) + a- F~- (0.5i x1 + 0.5 x2) - g3 D3 x1 x2 F~ + (i n + b3 D3) P~
+#pragma unroll
+      for (int j2 = 0; j2 < N; ++j2) {
+        const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
+        const int o = j2 * (N + 1) + j1;
+        const C vp = fp[o], vm = fm[o];
+        C y;
+        // a+ vp * (0.5 i x1 - 0.5 x2) + a- vm * (0.5 i x1 + 0.5 x2)
+        const T h1 = (T)0.5 * x1, h2 = (T)0.5 * x2;
+        y.x = ap * (-h1 * vp.y - h2 * vp.x) + am * (-h1 * vm.y + h2 * vm.x);
+        y.y = ap * (h1 * vp.x - h2 * vp.y) + am * (h1 * vm.x + h2 * vm.y);
+        if (HAS_P3) {
+          const C v0 = f0[o], pv = pp[o];
+          // - g3 (i d3) x1 x2 v0
+          const T s = g3 * d3 * x1 * x2;
+          y.x += s * v0.y;
+          y.y -= s * v0.x;
+          // (i n + b3 i d3) pv = i (n + b3 d3) pv
+          const T q = (T)n + b3 * d3;
+          y.x -= q * pv.y;
+          y.y += q * pv.x;
+        }
+        x[j2] = y;
+      }
+      fft<N, false>(x);
+#pragma unroll
+      for (int j = 0; j < N; ++j) sA[c * PS + j * (N + 1) + j1] = x[j];
+      // Y2 = b2 x2 F~ - g2 x1 P~  -> FFT_2 -> times D_2 = i d2(k2), added to A
+#pragma unroll
+      for (int j2 = 0; j2 < N; ++j2) {
+        const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
+        const int o = j2 * (N + 1) + j1;
+        C y = (b2 * x2) * f0[o];
+        if (HAS_P3) y = y - (g2 * x1) * pp[o];
+        x[j2] = y;
+      }
+      fft<N, false>(x);
+#pragma unroll
+      for (int k2 = 0; k2 < N; ++k2) {
+        const T dk = tp * (T)kappa_first(k2, N);
+        C* dst = sA + c * PS + k2 * (N + 1) + j1;
+        C v = *dst;
+        v.x -= dk * x[k2].y;
+        v.y += dk * x[k2].x;
+        *dst = v;
+      }
+    } else {
+      // Y1 = b1 x1 F~ - g1 x2 P~
+#pragma unroll
+      for (int j2 = 0; j2 < N; ++j2) {
+        const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
+        const int o = j2 * (N + 1) + j1;
+        C y = (b1 * x1) * f0[o];
+        if (HAS_P3) y = y - (g1 * x2) * pp[o];
+        x[j2] = y;
+      }
+      fft<N, false>(x);
+#pragma unroll
+      for (int j = 0; j < N; ++j) sY[c * PS + j * (N + 1) + j1] = x[j];
+    }
+  }
+  __syncthreads();
+
+  // ---- S5: forward FFT along k1; Y1' gets D_1 ----
+  for (int it = tid; it < tl.cnt * N * 2; it += nth) {
+    const int kind = it / (tl.cnt * N);
+    const int c = (it / N) % tl.cnt;
+    const int k2 = it % N;
+    C* pl = (kind == 0 ? sA : sY) + c * PS + k2 * (N + 1);
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = pl[j];
+    fft<N, false>(x);
+    if (kind == 0) {
+#pragma unroll
+      for (int j = 0; j < N; ++j) pl[j] = x[j];
+    } else {
+#pragma unroll
+      for (int k1 = 0; k1 < N; ++k1) {
+        const T dk = tp * (T)kappa_first(k1, N);
+        C v;
+        v.x = -dk * x[k1].y;
+        v.y = dk * x[k1].x;
+        pl[k1] = v;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- S6: dF = A + Y1' + G ; out = F0 + a dF ; acc += bacc dF ----
+  for (int e = tid; e < tl.cnt * N * N; e += nth) {
+    const int c = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
+    const long long r = row_of(L, tl.l, tl.m, tl.n0 + c);
+    const long long gi = r * L.nx + pbase + q;
+    const C s = sA[c * PS + k2 * (N + 1) + k1] + sY[c * PS + k2 * (N + 1) + k1];
+    const C g = Gl[gi];
+    const double dx = (double)s.x + (double)g.x, dy = (double)s.y + (double)g.y;
+    double2 o = F0 ? F0[gi] : make_double2(0.0, 0.0);
+    o.x += a * dx;
+    o.y += a * dy;
+    out[gi] = o;
+    if (acc) {
+      double2 v = acc[gi];
+      v.x += bacc * dx;
+      v.y += bacc * dy;
+      acc[gi] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ launcher ----
+template <typename T> static size_t plane_smem(int N, bool p3) {
+  const int C = PlaneCfg<T>::C;
+  const int planes = (C + 2) + (p3 ? C : 0) + 2 * C;
+  return (size_t)planes * N * (N + 1) * sizeof(c2<T>);
+}
+
+template <int N, typename T>
+static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
+                       double2* acc, double bacc, cudaStream_t s, const DerivParams& prm) {
+  using C = c2<T>;
+  int st = HP_OK;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  C* P3 = nullptr;
+  if (p->ndim == 3) {
+    P3 = (C*)p->ws_get("deriv.P3", fb, &st);
+    if (st) return st;
+  }
+  C* G = (C*)p->ws_get("deriv.G", fb, &st);
+  if (st) return st;
+  const RowLayout L = p->layout();
+  if (p->ndim == 3) {
+    const long long nt = p->nrows * (long long)N * N;
+    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  {
+    dim3 grid((unsigned)((p->nx + 127) / 128), (unsigned)p->nm);
+    k_local<T><<<grid, 128, 0, s>>>(L, Fev, G, p->tap_row, p->tap_w, prm);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  // tiles
+  constexpr int CT = PlaneCfg<T>::C;
+  static thread_local std::vector<PlaneTile> htiles;
+  htiles.clear();
+  for (int m = p->m_lo; m <= p->lmax; ++m)
+    for (int l = std::abs(m); l <= p->lmax; ++l)
+      for (int n0 = -l; n0 <= l; n0 += CT) htiles.push_back({m, l, n0, std::min(CT, l - n0 + 1)});
+  PlaneTile* dt = (PlaneTile*)p->ws_get(CT == 2 ? "deriv.tiles2" : "deriv.tiles4",
+                                        sizeof(PlaneTile) * htiles.size(), &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaMemcpyAsync(dt, htiles.data(), sizeof(PlaneTile) * htiles.size(),
+                              cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  const bool p3 = p->ndim == 3;
+  const size_t smem = plane_smem<T>(N, p3);
+  dim3 grid((unsigned)htiles.size(), p3 ? N : 1);
+  if (p3) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, true><<<grid, 256, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+  } else {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, false><<<grid, 256, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+template <typename T>
+static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
+                     double2* acc, double bacc, cudaStream_t s, const DerivParams& prm) {
+  switch (p->N) {
+    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    default:
+      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+// out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
+int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
+                       double2* acc, double bacc, cudaStream_t s) {
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  DerivParams prm;
+  prm.L = p->model.L;
+  for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; }
+  for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
+  if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
+  if (p->precision == HP_FP64) return run_deriv<double>(p, Fev, F0, a, out, acc, bacc, s, prm);
+  return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm);
+}

@@ -1,0 +1,94 @@
+// Plan: sizes, row layout, device tables and workspace of one (B, Bx, ndim,
+// precision, symmetry) configuration.
+#pragma once
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/hp.h"
+
+// Device-side view of the row layout, passed by value to kernels.
+//
+// Internal coefficient layout ("row-major over omega"): F[row * nx + w], where
+// w = k1 + N*k2 (+ N^2*k3) runs over the omega Fourier grid in FFT order and a
+// row is one (l, m, n) with m in [m_lo, lmax] (m_lo = 0 for HP_REAL, -lmax for
+// HP_COMPLEX), n in [-lmax, lmax] and l in [max(|m|,|n|), lmax], ordered by
+// m, then n, then l.  Rows of one (m, n) segment are therefore consecutive in l.
+struct RowLayout {
+  int B, lmax, N, ndim, m_lo, nm;   // nm = number of stored m values
+  long long nx, nrows;
+  const char4* rows;                // (l, m, n, 0) per row
+  const int* seg;                   // first row of segment (m, n): seg[(m-m_lo)*(2lmax+1) + n+lmax]
+};
+
+struct hp_state;
+
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct hp_plan {
+  int B = 0, lmax = 0, Bx = 0, N = 0, ndim = 0, precision = 0, symmetry = 0;
+  int m_lo = 0, nm = 0, D = 0;     // D = 2lmax+1
+  long long nx = 0, nrows = 0;
+  cudaStream_t stream = nullptr;
+
+  std::vector<char4> h_rows;
+  std::vector<int> h_seg;
+
+  // device tables
+  char4* rows = nullptr;
+  int* seg = nullptr;
+  double* wig64 = nullptr;   // [b][row] d^l_mn(beta_b)
+  float* wig32 = nullptr;
+  double* wfull = nullptr;   // d(2lmax+1,2lmax+1,lmax+1,2B) in the MATLAB layout
+  double* qw = nullptr;      // quadrature weights [2B]
+  double* cg1 = nullptr;     // <l1 m1; 1 m2 | l m> table, see cg1_index()
+
+  // model
+  bool has_model = false;
+  hp_model model{};
+  int* tap_row = nullptr;    // [row][9]  (-1 = no tap)
+  double2* tap_w = nullptr;  // [ndim][row][9]
+
+  // workspace (grow-only), keyed by name
+  std::vector<std::pair<std::string, Buf>> ws;
+  void* ws_get(const char* name, size_t bytes, int* status);
+
+  RowLayout layout() const {
+    RowLayout L;
+    L.B = B; L.lmax = lmax; L.N = N; L.ndim = ndim; L.m_lo = m_lo; L.nm = nm;
+    L.nx = nx; L.nrows = nrows; L.rows = rows; L.seg = seg;
+    return L;
+  }
+  size_t cplx_bytes() const { return precision == HP_FP64 ? 16 : 8; }
+  long long n_full() const { return (long long)D * D * (lmax + 1) * nx; }
+  long long n_grid() const { return 8LL * B * B * B * nx; }
+};
+
+struct hp_state {
+  hp_plan* plan = nullptr;
+  double2* F = nullptr;     // current coefficients, FP64, internal layout
+  double2* F2 = nullptr;    // ping-pong / stage buffers
+  double2* F3 = nullptr;
+  double2* acc = nullptr;
+};
+
+// <l1 m1; 1 m2 | l m> with m1 = m - m2, l = l1 + dl (dl in -1..1):
+// cg1[((l1 * 3 + (dl+1)) * (2*lmax+3) + (m + lmax+1)) * 3 + (m2+1)]
+inline __host__ __device__ int cg1_index(int lmax, int l1, int dl, int m, int m2) {
+  return ((l1 * 3 + (dl + 1)) * (2 * lmax + 3) + (m + lmax + 1)) * 3 + (m2 + 1);
+}
+
+// ---- launchers implemented in the .cu files (return hp_status) ----
+int hp_tables_build(hp_plan* p);
+int hp_twiddles_init();
+int hp_build_gravity_taps(hp_plan* p, const double2* MR_full_dev);
+int hp_full_to_internal(hp_plan* p, const double2* Ffull, double2* Fint, cudaStream_t s);
+int hp_internal_to_full(hp_plan* p, const double2* Fint, double2* Ffull, cudaStream_t s);
+int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, double a,
+                       double2* out, double2* acc, double bacc, cudaStream_t s);
+int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s);
+int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s);
+int hp_prod_launch(hp_plan* p, const double2* F, const double2* G, double2* FG, int batch,
+                   cudaStream_t s);

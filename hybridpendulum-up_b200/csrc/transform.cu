@@ -1,0 +1,507 @@
+// SO(3) x R^n transforms (fftSO3R forward / backward) on the internal layout.
+//
+// Backward (ifftSO3R.m:16-37, pendulum.m:284-304):
+//   1. inverse omega FFT of every coefficient row (plane pass over (k1,k2),
+//      line pass over k3), normalised by 1/nx  -> rows x physical omega;
+//   2. transpose to omega-major so each omega point's coefficients are contiguous;
+//   3. synthesis per omega point and beta_b:
+//        G_b[m][n] = sum_l (2l+1) d^l_mn(beta_b) F^l_mn
+//        H_b[m][c] = sum_n G_b[m][n] e^{-i n gamma_c}          (2B-point FFT)
+//        f[a][b][c] = sum_m H_b[m][c] e^{-i m alpha_a}          (2B-point FFT)
+//      For HP_REAL plans only m >= 0 is stored and f = Re(H_0 + 2 sum_{m>0} ...),
+//      the Hermitian reconstruction of ifftn(..., 'symmetric').
+// Forward (fftSO3R.m:89-106) runs the same stages in reverse with the
+// quadrature weights w_b.
+#include <vector>
+#include "common.cuh"
+#include "plan.hpp"
+
+using namespace hp;
+
+// ------------------------------------------------------------ omega FFTs ----
+// 2-D FFT over (k1, k2) of every (row, k3) plane; one block per (row, k3).
+template <int N, typename Tin, typename T, bool INV>
+__global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, c2<T>* __restrict__ out,
+                                                long long nplanes, T scale) {
+  using C = c2<T>;
+  __shared__ C sm[N * (N + 1)];
+  const long long pl = blockIdx.x;
+  if (pl >= nplanes) return;
+  const c2<Tin>* src = in + pl * N * N;
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x)
+    sm[(e / N) * (N + 1) + e % N] = cvt<C, c2<Tin>>(src[e]);
+  __syncthreads();
+  for (int k2 = threadIdx.x; k2 < N; k2 += blockDim.x) {
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = sm[k2 * (N + 1) + j];
+    fft<N, INV>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) sm[k2 * (N + 1) + j] = x[j];
+  }
+  __syncthreads();
+  for (int k1 = threadIdx.x; k1 < N; k1 += blockDim.x) {
+    C x[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = sm[j * (N + 1) + k1];
+    fft<N, INV>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) sm[j * (N + 1) + k1] = scale * x[j];
+  }
+  __syncthreads();
+  C* dst = out + pl * N * N;
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x) dst[e] = sm[(e / N) * (N + 1) + e % N];
+}
+
+// 1-D FFT along the last omega axis (stride N^2) of a [row][N^3] array.
+template <int N, typename T, bool INV>
+__global__ void __launch_bounds__(128) k_wline(const c2<T>* __restrict__ in, c2<T>* __restrict__ out,
+                                               long long nrows, T scale) {
+  using C = c2<T>;
+  constexpr long long plane = (long long)N * N;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= nrows * plane) return;
+  const long long row = t / plane, p = t % plane;
+  const C* src = in + row * plane * N + p;
+  C x[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) x[j] = src[j * plane];
+  fft<N, INV>(x);
+  C* dst = out + row * plane * N + p;
+#pragma unroll
+  for (int j = 0; j < N; ++j) dst[j * plane] = scale * x[j];
+}
+
+// out[c][r] = in[r][c] for an R x Cc matrix of complex T (32x32 tiles).
+template <typename Tin, typename Tout>
+__global__ void k_transpose(const c2<Tin>* __restrict__ in, c2<Tout>* __restrict__ out, long long R,
+                            long long Cc) {
+  __shared__ c2<Tout> tile[32][33];
+  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const long long r = r0 + k, c = c0 + threadIdx.x;
+    if (r < R && c < Cc) tile[k][threadIdx.x] = cvt<c2<Tout>, c2<Tin>>(in[r * Cc + c]);
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const long long c = c0 + k, r = r0 + threadIdx.x;
+    if (r < R && c < Cc) out[c * R + r] = tile[threadIdx.x][k];
+  }
+}
+
+// ------------------------------------------------------------ synthesis ----
+// Block = (group of NB consecutive beta indices, range of omega points);
+// the d values of its betas stay in shared memory.  P omega points per batch.
+template <int B, typename T, int NB, bool CPLX>
+__global__ void __launch_bounds__(512) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
+                                               const T* __restrict__ wig, void* __restrict__ fout,
+                                               int P, long long w_per_block) {
+  using C = c2<T>;
+  constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
+  constexpr int NM = CPLX ? D : B;          // stored m values
+  constexpr int MLO = CPLX ? -lmax : 0;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sd = reinterpret_cast<T*>(smraw);                       // [NB][nrows]
+  size_t off = ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
+  C* sG = reinterpret_cast<C*>(smraw + off);                 // [P][NB][NM][NB2]
+  const int b0 = blockIdx.y * NB;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (long long e = tid; e < (long long)NB * L.nrows; e += nth) {
+    const int bb = (int)(e / L.nrows);
+    sd[e] = (b0 + bb < NB2) ? wig[(long long)(b0 + bb) * L.nrows + e % L.nrows] : (T)0;
+  }
+  const long long wbeg = blockIdx.x * w_per_block;
+  const long long wend = min(wbeg + w_per_block, L.nx);
+  const int npairs = NM * D;
+  for (long long w0 = wbeg; w0 < wend; w0 += P) {
+    const int pc = (int)min((long long)P, wend - w0);
+    __syncthreads();
+    // beta stage
+    for (int it = tid; it < pc * npairs; it += nth) {
+      const int p = it / npairs, pr = it % npairs;
+      const int mi = pr / D, n = pr % D - lmax, m = mi + MLO;
+      const int am = abs(m), an = abs(n), lmin = am > an ? am : an;
+      const int q = n >= 0 ? n : n + NB2;
+      C* g = sG + ((size_t)p * NB * NM + mi) * NB2;
+      if (n == 0)
+        for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + B] = czero<C>();
+      if (lmin > lmax) {
+        for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + q] = czero<C>();
+        continue;
+      }
+      const long long s = L.seg[(m - L.m_lo) * D + n + lmax];
+      C acc[NB];
+#pragma unroll
+      for (int bb = 0; bb < NB; ++bb) acc[bb] = czero<C>();
+      const C* src = Fp + (w0 + p) * L.nrows + s;
+      for (int j = 0; j <= lmax - lmin; ++j) {
+        const C v = src[j];
+        const T l2 = (T)(2 * (lmin + j) + 1);
+#pragma unroll
+        for (int bb = 0; bb < NB; ++bb) {
+          const T dv = l2 * sd[(size_t)bb * L.nrows + s + j];
+          acc[bb].x += dv * v.x;
+          acc[bb].y += dv * v.y;
+        }
+      }
+#pragma unroll
+      for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + q] = acc[bb];
+    }
+    __syncthreads();
+    // gamma stage: rows (p, bb, mi) over n -> c
+    for (int it = tid; it < pc * NB * NM; it += nth) {
+      C* g = sG + (size_t)it * NB2;
+      C x[NB2];
+#pragma unroll
+      for (int j = 0; j < NB2; ++j) x[j] = g[j];
+      fft<NB2, false>(x);
+#pragma unroll
+      for (int j = 0; j < NB2; ++j) g[j] = x[j];
+    }
+    __syncthreads();
+    // alpha stage: (p, bb, c) over m -> a ; single round (host guarantees pc*NB*NB2 <= nth)
+    const int nalpha = pc * NB * NB2;
+    const bool act = tid < nalpha;
+    C x[NB2];
+    int p = 0, bb = 0, c = 0;
+    if (act) {
+      p = tid / (NB * NB2);
+      bb = (tid / NB2) % NB;
+      c = tid % NB2;
+      const C* h = sG + ((size_t)(p * NB + bb) * NM) * NB2 + c;
+#pragma unroll
+      for (int q = 0; q < NB2; ++q) x[q] = czero<C>();
+      if (CPLX) {
+#pragma unroll
+        for (int mi = 0; mi < NM; ++mi) {
+          const int m = mi + MLO;
+          x[m >= 0 ? m : m + NB2] = h[(size_t)mi * NB2];
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < NM; ++m) x[m] = (m == 0 ? (T)1 : (T)2) * h[(size_t)m * NB2];
+      }
+      fft<NB2, false>(x);
+    }
+    __syncthreads();
+    if (act) {
+      // stage into sG as [p][c][bb][a]
+      if (CPLX) {
+        C* st = sG + (((size_t)p * NB2 + c) * NB + bb) * NB2;
+#pragma unroll
+        for (int a = 0; a < NB2; ++a) st[a] = x[a];
+      } else {
+        T* st = reinterpret_cast<T*>(sG) + (((size_t)p * NB2 + c) * NB + bb) * NB2;
+#pragma unroll
+        for (int a = 0; a < NB2; ++a) st[a] = x[a].x;
+      }
+    }
+    __syncthreads();
+    // coalesced store: f[a + 2B (b + 2B (c + 2B w))]
+    const int nbv = min(NB, NB2 - b0);
+    const long long per_w = (long long)NB2 * nbv * NB2;
+    for (long long e = tid; e < (long long)pc * per_w; e += nth) {
+      const int pp = (int)(e / per_w);
+      const int r = (int)(e % per_w);
+      const int cc = r / (nbv * NB2), bq = (r / NB2) % nbv, a = r % NB2;
+      const long long gi = (long long)a + NB2 * ((long long)(b0 + bq) + NB2 * ((long long)cc + NB2 * (w0 + pp)));
+      const size_t si = (((size_t)pp * NB2 + cc) * NB + bq) * NB2 + a;
+      if (CPLX) reinterpret_cast<C*>(fout)[gi] = sG[si];
+      else reinterpret_cast<T*>(fout)[gi] = reinterpret_cast<T*>(sG)[si];
+    }
+  }
+}
+
+// ------------------------------------------------------------- analysis ----
+// Block = (group of NB betas, range of omega points).  Per omega point:
+//   alpha stage  Q1[c][m] = sum_a f[a][b][c] e^{+i m alpha_a}
+//   gamma stage  Q[m][n]  = sum_c Q1[c][m] e^{+i n gamma_c}
+//   beta  stage  Fa[w][(m,n,l)] += sum_b w_b d^l_mn(beta_b) Q_b[m][n]
+// The beta sum over groups of betas is accumulated with atomics.
+template <int B, typename T, int NB, bool CPLX>
+__global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restrict__ fin,
+                                              const T* __restrict__ wig, const double* __restrict__ qw,
+                                              c2<T>* __restrict__ Fa, int P, long long w_per_block) {
+  using C = c2<T>;
+  constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
+  constexpr int NM = CPLX ? D : B;
+  constexpr int MLO = CPLX ? -lmax : 0;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sd = reinterpret_cast<T*>(smraw);  // [NB][nrows] w_b d
+  size_t off = ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
+  C* sQ = reinterpret_cast<C*>(smraw + off);  // [P][NB][NM][NB2] (n bins)
+  size_t off2 = off + (size_t)P * NB * NM * NB2 * sizeof(C);
+  C* sIn = reinterpret_cast<C*>(smraw + off2);  // [P][NB][NB2 (c)][NB2 (a)]
+  const int b0 = blockIdx.y * NB;
+  const int nbv = min(NB, NB2 - b0);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (long long e = tid; e < (long long)NB * L.nrows; e += nth) {
+    const int bb = (int)(e / L.nrows);
+    sd[e] = (bb < nbv) ? (T)(qw[b0 + bb] * (double)wig[(long long)(b0 + bb) * L.nrows + e % L.nrows]) : (T)0;
+  }
+  const long long wbeg = blockIdx.x * w_per_block;
+  const long long wend = min(wbeg + w_per_block, L.nx);
+  for (long long w0 = wbeg; w0 < wend; w0 += P) {
+    const int pc = (int)min((long long)P, wend - w0);
+    __syncthreads();
+    // load f lines into sIn[p][bb][c][a]
+    const long long per_w = (long long)NB2 * nbv * NB2;
+    for (long long e = tid; e < (long long)pc * per_w; e += nth) {
+      const int pp = (int)(e / per_w), r = (int)(e % per_w);
+      const int cc = r / (nbv * NB2), bq = (r / NB2) % nbv, a = r % NB2;
+      const long long gi = (long long)a + NB2 * ((long long)(b0 + bq) + NB2 * ((long long)cc + NB2 * (w0 + pp)));
+      C v;
+      if (CPLX) v = reinterpret_cast<const C*>(fin)[gi];
+      else { v.x = reinterpret_cast<const T*>(fin)[gi]; v.y = 0; }
+      sIn[(((size_t)pp * NB + bq) * NB2 + cc) * NB2 + a] = v;
+    }
+    __syncthreads();
+    // alpha stage: item (p, bb, c): FFT(+) over a, keep stored m bins -> sQ[p][bb][mi][c]
+    for (int it = tid; it < pc * nbv * NB2; it += nth) {
+      const int pp = it / (nbv * NB2), bq = (it / NB2) % nbv, cc = it % NB2;
+      const C* src = sIn + (((size_t)pp * NB + bq) * NB2 + cc) * NB2;
+      C x[NB2];
+#pragma unroll
+      for (int a = 0; a < NB2; ++a) x[a] = src[a];
+      fft<NB2, true>(x);
+      C* dst = sQ + ((size_t)(pp * NB + bq) * NM) * NB2 + cc;
+#pragma unroll
+      for (int mi = 0; mi < NM; ++mi) {
+        const int m = mi + MLO;
+        dst[(size_t)mi * NB2] = x[m >= 0 ? m : m + NB2];
+      }
+    }
+    __syncthreads();
+    // gamma stage: item (p, bb, mi): FFT(+) over c, in place (bins n mod 2B)
+    for (int it = tid; it < pc * nbv * NM; it += nth) {
+      const int pp = it / (nbv * NM), bq = (it / NM) % nbv, mi = it % NM;
+      C* row = sQ + ((size_t)(pp * NB + bq) * NM + mi) * NB2;
+      C x[NB2];
+#pragma unroll
+      for (int j = 0; j < NB2; ++j) x[j] = row[j];
+      fft<NB2, true>(x);
+#pragma unroll
+      for (int j = 0; j < NB2; ++j) row[j] = x[j];
+    }
+    __syncthreads();
+    // beta stage: item (p, m, n): sum over the group's betas, atomically added
+    const int npairs = NM * D;
+    for (int it = tid; it < pc * npairs; it += nth) {
+      const int pp = it / npairs, pr = it % npairs;
+      const int mi = pr / D, n = pr % D - lmax, m = mi + MLO;
+      const int am = abs(m), an = abs(n), lmin = am > an ? am : an;
+      if (lmin > lmax) continue;
+      const int q = n >= 0 ? n : n + NB2;
+      const long long s = L.seg[(m - L.m_lo) * D + n + lmax];
+      C* dst = Fa + (w0 + pp) * L.nrows + s;
+      for (int j = 0; j <= lmax - lmin; ++j) {
+        C acc = czero<C>();
+        for (int bq = 0; bq < nbv; ++bq) {
+          const T dv = sd[(size_t)bq * L.nrows + s + j];
+          const C v = sQ[((size_t)(pp * NB + bq) * NM + mi) * NB2 + q];
+          acc.x += dv * v.x;
+          acc.y += dv * v.y;
+        }
+        atomicAdd(&dst[j].x, acc.x);
+        atomicAdd(&dst[j].y, acc.y);
+      }
+    }
+  }
+}
+
+// -------------------------------------------------------------- drivers ----
+template <typename T> struct TfCfg;
+template <> struct TfCfg<double> { static constexpr int NB = 2; static constexpr int threads = 256; };
+template <> struct TfCfg<float> { static constexpr int NB = 4; static constexpr int threads = 512; };
+
+static int smem_limit() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return v;
+}
+
+template <int N, typename Tin, typename T>
+static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s) {
+  // in/out [row][nx]; in may equal out only when Tin == T
+  const T scale = inv ? (T)1 / (T)p->nx : (T)1;
+  const long long nplanes = p->nrows * (p->ndim == 3 ? N : 1);
+  if (p->ndim == 3) {
+    // plane pass (k1,k2) then line pass along k3, scale applied in the line pass
+    if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
+    else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
+    HP_CUDA_TRY(cudaGetLastError());
+    const long long nt = p->nrows * (long long)N * N;
+    if (inv) k_wline<N, T, true><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
+    else k_wline<N, T, false><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
+  } else {
+    if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
+    else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+template <typename Tin, typename T>
+static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s) {
+  switch (p->N) {
+    case 4: return omega_fft<4, Tin, T>(p, in, out, inv, s);
+    case 6: return omega_fft<6, Tin, T>(p, in, out, inv, s);
+    case 8: return omega_fft<8, Tin, T>(p, in, out, inv, s);
+    case 12: return omega_fft<12, Tin, T>(p, in, out, inv, s);
+    case 16: return omega_fft<16, Tin, T>(p, in, out, inv, s);
+    case 20: return omega_fft<20, Tin, T>(p, in, out, inv, s);
+    case 24: return omega_fft<24, Tin, T>(p, in, out, inv, s);
+    case 32: return omega_fft<32, Tin, T>(p, in, out, inv, s);
+    default:
+      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+template <int B, typename T, bool CPLX>
+static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
+  using C = c2<T>;
+  constexpr int NB = TfCfg<T>::NB, NB2 = 2 * B;
+  constexpr int NM = CPLX ? 2 * B - 1 : B;
+  const int threads = TfCfg<T>::threads;
+  const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
+  const size_t per_p = std::max((size_t)NB * NM * NB2 * sizeof(C),
+                                (size_t)NB * NB2 * NB2 * (CPLX ? sizeof(C) : sizeof(T)));
+  const int lim = smem_limit();
+  int P = std::max(1, threads / (NB * NB2));
+  while (P > 1 && sd_bytes + P * per_p > (size_t)lim) --P;
+  if (sd_bytes + P * per_p > (size_t)lim) {
+    hp_set_error("synthesis tables exceed shared memory for this bandlimit");
+    return HP_ERR_UNSUPPORTED;
+  }
+  const size_t smem = sd_bytes + P * per_p;
+  const int ngroups = (NB2 + NB - 1) / NB;
+  // enough blocks to fill the machine several times over
+  long long wblocks = std::max(1LL, std::min(p->nx, 8LL * 148 * 2 / ngroups + 1));
+  long long wpb = (p->nx + wblocks - 1) / wblocks;
+  wpb = (wpb + P - 1) / P * P;
+  wblocks = (p->nx + wpb - 1) / wpb;
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((unsigned)wblocks, (unsigned)ngroups);
+  k_synth<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), Fp,
+                                                       p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
+                                                                               : (const T*)(const void*)p->wig32,
+                                                       f, P, wpb);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+template <int B, typename T, bool CPLX>
+static int anal_launch(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
+  using C = c2<T>;
+  constexpr int NB = TfCfg<T>::NB, NB2 = 2 * B;
+  constexpr int NM = CPLX ? 2 * B - 1 : B;
+  const int threads = TfCfg<T>::threads;
+  const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
+  const size_t per_p = (size_t)NB * NM * NB2 * sizeof(C) + (size_t)NB * NB2 * NB2 * sizeof(C);
+  const int lim = smem_limit();
+  int P = 4;
+  while (P > 1 && sd_bytes + P * per_p > (size_t)lim) --P;
+  if (sd_bytes + P * per_p > (size_t)lim) {
+    hp_set_error("analysis tables exceed shared memory for this bandlimit");
+    return HP_ERR_UNSUPPORTED;
+  }
+  const size_t smem = sd_bytes + P * per_p;
+  const int ngroups = (NB2 + NB - 1) / NB;
+  long long wblocks = std::max(1LL, std::min(p->nx, 8LL * 148 * 2 / ngroups + 1));
+  long long wpb = (p->nx + wblocks - 1) / wblocks;
+  wpb = (wpb + P - 1) / P * P;
+  wblocks = (p->nx + wpb - 1) / wpb;
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_anal<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((unsigned)wblocks, (unsigned)ngroups);
+  HP_CUDA_TRY(cudaMemsetAsync(Fa, 0, sizeof(C) * p->nrows * p->nx, s));
+  k_anal<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), f,
+                                                      p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
+                                                                              : (const T*)(const void*)p->wig32,
+                                                      p->qw, Fa, P, wpb);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+#define HP_FOR_EACH_B(X) X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(32)
+
+template <typename T, bool CPLX>
+static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
+  switch (p->B) {
+#define X(b) case b: return synth_launch<b, T, CPLX>(p, Fp, f, s);
+    HP_FOR_EACH_B(X)
+#undef X
+    default:
+      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+template <typename T, bool CPLX>
+static int anal_any(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
+  switch (p->B) {
+#define X(b) case b: return anal_launch<b, T, CPLX>(p, f, Fa, s);
+    HP_FOR_EACH_B(X)
+#undef X
+    default:
+      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+template <typename T>
+static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s) {
+  using C = c2<T>;
+  int st = HP_OK;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  C* t1 = (C*)p->ws_get("tf.t1", fb, &st);
+  if (st) return st;
+  C* t2 = (C*)p->ws_get("tf.t2", fb, &st);
+  if (st) return st;
+  st = omega_fft_any<double, T>(p, Fint, t1, true, s);
+  if (st) return st;
+  dim3 grid((unsigned)((p->nx + 31) / 32), (unsigned)((p->nrows + 31) / 32));
+  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nrows, p->nx);
+  HP_CUDA_TRY(cudaGetLastError());
+  if (complex_out) return synth_any<T, true>(p, t2, f, s);
+  return synth_any<T, false>(p, t2, f, s);
+}
+
+template <typename T>
+static int forward_T(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {
+  using C = c2<T>;
+  int st = HP_OK;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  C* t1 = (C*)p->ws_get("tf.t1", fb, &st);
+  if (st) return st;
+  C* t2 = (C*)p->ws_get("tf.t2", fb, &st);
+  if (st) return st;
+  st = complex_in ? anal_any<T, true>(p, f, t1, s) : anal_any<T, false>(p, f, t1, s);
+  if (st) return st;
+  dim3 grid((unsigned)((p->nrows + 31) / 32), (unsigned)((p->nx + 31) / 32));
+  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nx, p->nrows);
+  HP_CUDA_TRY(cudaGetLastError());
+  st = omega_fft_any<T, T>(p, t2, t1, false, s);
+  if (st) return st;
+  // to FP64 rows
+  const long long n = p->nrows * p->nx;
+  dim3 g2((unsigned)((n + 31) / 32), 1);
+  // reuse the transpose kernel as a converter (1 x n matrix)
+  dim3 gridc((unsigned)((n + 31) / 32), 1);
+  k_transpose<T, double><<<gridc, dim3(32, 8), 0, s>>>(t1, Fint, 1, n);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  if (p->precision == HP_FP64) return backward_T<double>(p, Fint, f, complex_out, s);
+  return backward_T<float>(p, Fint, f, complex_out, s);
+}
+
+int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  if (p->precision == HP_FP64) return forward_T<double>(p, f, complex_in, Fint, s);
+  return forward_T<float>(p, f, complex_in, Fint, s);
+}

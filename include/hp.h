@@ -1,0 +1,147 @@
+/*
+ * hp.h -- C ABI of the B200 (sm_100a) Fokker-Planck propagation library for
+ * densities on SO(3) x R^n (n = 2 or 3).
+ *
+ * Each entry point replaces one MEX gateway or MATLAB function of the reference
+ * (fdcl-gwu/hybridPendulum-UP); the citation is on each declaration.  All
+ * entry points return an int status (HP_OK == 0); hp_last_error() gives a
+ * message for the last failure on the calling thread.
+ *
+ * Array arguments use the reference's MATLAB layouts (column-major, complex
+ * values interleaved re/im as in the R2018a MEX API):
+ *   F  (2lmax+1, 2lmax+1, lmax+1, 2Bx, 2Bx[, 2Bx])  complex, F(m+lmax+1, n+lmax+1, l+1, i, j, k)
+ *   f  (2B, 2B, 2B, 2Bx, 2Bx[, 2Bx])                real (or complex), f(alpha, beta, gamma, i, j, k)
+ *   MR (2lmax+1, 2lmax+1, lmax+1, n)                complex
+ * with lmax = B-1.  `mem` says where a pointer lives (HP_DEVICE or HP_HOST);
+ * host pointers are staged through the plan's device workspace.
+ */
+#ifndef HP_H
+#define HP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum hp_status {
+  HP_OK = 0,
+  HP_ERR_INVALID = 1,     /* null pointer, bad enum, bad size            */
+  HP_ERR_SHAPE = 2,       /* sizes inconsistent with the plan            */
+  HP_ERR_ALLOC = 3,       /* device or host allocation failed            */
+  HP_ERR_CUDA = 4,        /* a CUDA call failed                          */
+  HP_ERR_UNSUPPORTED = 5, /* input outside the supported model class     */
+  HP_ERR_NONFINITE = 6,   /* a NaN/Inf guard fired                       */
+  HP_ERR_NO_MODEL = 7     /* propagation requested before hp_plan_set_model */
+};
+
+enum hp_precision {
+  HP_FP64 = 0,  /* every kernel in FP64                                           */
+  HP_MIXED = 1  /* FP32 operators / transforms, FP64 coefficient accumulation     */
+};
+
+enum hp_symmetry {
+  HP_REAL = 0,    /* coefficients of a real density: only m >= 0 rows are stored,
+                     m < 0 follow from F^l_{-m,-n}[-k] = (-1)^(m-n) conj F^l_{mn}[k] */
+  HP_COMPLEX = 1  /* general complex coefficients: every (l, m, n) row is stored     */
+};
+
+enum hp_method { HP_EULER = 0, HP_MIDPOINT = 1, HP_RK2 = 2, HP_RK4 = 3 };
+enum hp_mem { HP_DEVICE = 0, HP_HOST = 1 };
+
+typedef struct hp_plan hp_plan;
+typedef struct hp_state hp_state;
+
+/* Sizes of a plan (all counts are elements, bytes are device bytes). */
+typedef struct {
+  int B, lmax, Bx, N, ndim, precision, symmetry;
+  long long nx;          /* (2Bx)^ndim                                    */
+  long long nrows;       /* stored (l, m, n) rows                         */
+  long long n_full;      /* elements of the full MATLAB F layout          */
+  long long n_grid;      /* elements of the f grid: (2B)^3 * nx           */
+  long long state_bytes; /* device bytes of one resident coefficient state */
+} hp_plan_info_t;
+
+/*
+ * Pendulum model: the derivative inputs of the reference MEX
+ * pendulum_propagate(F,X,OJO,MR,bt,G,dt,L,u,CG,method)
+ * (propagation/mex/sources/pendulum_propagate/kernel.cu:16-76).
+ *   L      omega-grid period: x_i = -L/2 + L*j/(2Bx)            (pendulum.m:90-99)
+ *   b      damping: Omega-dot contains -b_i Omega_i               (pendulum.m:424-427)
+ *   G      noise matrix G = H H^T / 2, row-major 3x3 (ndim x ndim used)  (pendulum.m:202-208)
+ *   gyro   J^-1(-Omega x J Omega) for diagonal J written as
+ *          (gyro0*O2*O3, gyro1*O1*O3, gyro2*O1*O2)             (pendulum.m:145-158)
+ * X and OJO of the MEX are functions of (L, J) and are rebuilt from them;
+ * u and CG are plan tables.  MR is passed to hp_plan_set_model.
+ */
+typedef struct {
+  double L;
+  double b[3];
+  double G[9];
+  double gyro[3];
+} hp_model;
+
+/* Plan: tables (Wigner-d, quadrature weights, Clebsch-Gordan, twiddles) are
+ * built on the device in FP64.  Replaces the per-call setup of every MEX
+ * (e.g. propagation/mex/sources/fftSO3R/kernel.cu:20-130) and the MATLAB table
+ * builders Wigner_d.m:1-47, getu.m:132-163, clebsch_gordan.m:1-43. */
+int hp_plan_create(hp_plan** plan, int B, int Bx, int ndim, int precision, int symmetry);
+int hp_plan_destroy(hp_plan* plan);
+int hp_plan_get_info(const hp_plan* plan, hp_plan_info_t* info);
+/* Stream for every launch of this plan (a cudaStream_t; NULL = legacy default). */
+int hp_plan_set_stream(hp_plan* plan, void* cuda_stream);
+const char* hp_last_error(void);
+
+/* Model for the propagation entry points.  MR: complex (2lmax+1,2lmax+1,lmax+1,ndim)
+ * in the full layout; only its degree-1, m2=0 block may be non-zero (the
+ * gravity term of pendulum.m:166-192 depends on R through R^T e3 only);
+ * otherwise HP_ERR_UNSUPPORTED. */
+int hp_plan_set_model(hp_plan* plan, const hp_model* model, const double* MR, int mem);
+
+/* Copy of the plan's Wigner-d table d(2lmax+1, 2lmax+1, lmax+1, 2B) in the
+ * layout of pendulum.m:107-111 (d(m+lmax+1, n+lmax+1, l+1, j)); out is FP64. */
+int hp_wigner_d(hp_plan* plan, double* d, int mem);
+/* Quadrature weights w(2B) of fftSO3R.m:62-66. */
+int hp_quad_weights(hp_plan* plan, double* w, int mem);
+
+/* Forward transform F = fftSO3R(f): replaces fftSO3R_mex('forward', f, d, w)
+ * (propagation/mex/sources/fftSO3R/kernel.cu:11-195) and fftSO3R.m:89-106.
+ * f real (HP_REAL plans) or complex interleaved (HP_COMPLEX plans). */
+int hp_fftSO3R_forward(hp_plan* plan, const double* f, double* F, int mem);
+/* Backward transform f = ifftSO3R(F): replaces fftSO3R_mex('backward', F, d)
+ * (kernel.cu:196-391), ifftSO3R.m:16-37 and the inline pendulum.m:284-304. */
+int hp_fftSO3R_backward(hp_plan* plan, const double* F, double* f, int mem);
+
+/* One propagation step Fnew = integrate(Fold): replaces
+ * pendulum_propagate (ndim=3, propagation/mex/sources/pendulum_propagate/kernel.cu:9-519)
+ * and pendulum_propagate_reduced (ndim=2, .../pendulum_propagate_reduced/kernel.cu:9-262),
+ * i.e. the integrate/derivative pair of pendulum.m:346-527 and
+ * pendulum_reduced.m:320-465.  method: HP_EULER/MIDPOINT/RK2/RK4. */
+int hp_pendulum_propagate(hp_plan* plan, const double* Fold, double* Fnew, double dt,
+                          int method, int mem);
+/* The derivative dF of pendulum.m:388-527 / pendulum_reduced.m:362-465. */
+int hp_pendulum_derivative(hp_plan* plan, const double* F, double* dF, int mem);
+
+/* Product rule of fftSO3_prod.m:209-265 (complex branch), batched over `batch`
+ * independent pairs: FG^l = sum (2l1+1)(2l2+1)/(2l+1) [CG^T (F^l1 kron G^l2) CG]_l.
+ * F, G, FG: (2lmax+1, 2lmax+1, lmax+1, batch) complex. */
+int hp_fftSO3_prod(hp_plan* plan, const double* F, const double* G, double* FG, int batch,
+                   int mem);
+
+/* ---- resident state: coefficients kept on the device in the plan's internal
+ * layout across steps (the time loops of pendulum.m:269-315 and
+ * pendulum_reduced.m:243-289 without host round trips). ---- */
+int hp_state_create(hp_plan* plan, hp_state** state);
+int hp_state_destroy(hp_state* state);
+int hp_state_load(hp_state* state, const double* F, int mem);   /* full layout in  */
+int hp_state_store(hp_state* state, double* F, int mem);        /* full layout out */
+/* nsteps steps of `method` with step dt. */
+int hp_state_step(hp_state* state, double dt, int method, int nsteps);
+/* Density on the grid f = ifftSO3R(F) of the current state into `f`
+ * (device pointer; double for HP_FP64 plans, float for HP_MIXED plans). */
+int hp_state_density(hp_state* state, void* f);
+/* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
+int hp_state_mass(hp_state* state, double* mass);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HP_H */
