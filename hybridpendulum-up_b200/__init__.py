@@ -38,7 +38,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_fftSO3R_forward', 'hp_fftSO3R_backward', 'hp_pendulum_propagate',
            'hp_pendulum_derivative', 'hp_fftSO3_prod', 'hp_state_create', 'hp_state_destroy',
            'hp_state_load', 'hp_state_store', 'hp_state_step', 'hp_state_density',
-           'hp_state_mass']
+           'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count']
 
 
 class HPError(RuntimeError):
@@ -76,6 +76,9 @@ def _load():
         'hp_state_create': [vp, ctypes.POINTER(vp)], 'hp_state_destroy': [vp],
         'hp_state_load': [vp, vp, ip], 'hp_state_store': [vp, vp, ip],
         'hp_state_step': [vp, dp, ip, ip], 'hp_state_density': [vp, vp], 'hp_state_mass': [vp, ctypes.POINTER(dp)],
+        'hp_plan_profile': [vp, ip],
+        'hp_plan_profile_get': [vp, ip, ctypes.c_char_p, ip, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)],
+        'hp_plan_launch_count': [vp, ctypes.POINTER(ctypes.c_longlong)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -170,6 +173,27 @@ class Plan:
         _check(_lib.hp_plan_set_model(self._h, ctypes.byref(m), ctypes.c_void_p(p), mem))
         self.model = dict(L=float(L), b=np.array(bb[:3]), G=Gm, gyro=tuple(gyro))
         self._MR_keep = MRc
+
+    def profile(self, enable: bool = True):
+        """Start (and reset) or stop per-kernel-family CUDA-event timing."""
+        _check(_lib.hp_plan_profile(self._h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """{family: (total_ms, launches)} since the last profile(True)."""
+        out, i = {}, 0
+        buf = ctypes.create_string_buffer(64)
+        while True:
+            ms, cnt = ctypes.c_double(), ctypes.c_longlong()
+            if _lib.hp_plan_profile_get(self._h, i, buf, 64, ctypes.byref(ms), ctypes.byref(cnt)) != HP_OK:
+                break
+            out[buf.value.decode()] = (ms.value, cnt.value)
+            i += 1
+        return out
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        _check(_lib.hp_plan_launch_count(self._h, ctypes.byref(v)))
+        return v.value
 
     def wigner_d(self) -> np.ndarray:
         d = np.zeros((2 * self.lmax + 1, 2 * self.lmax + 1, self.lmax + 1, 2 * self.B), order='F')

@@ -46,6 +46,71 @@ void* hp_plan::ws_get(const char* name, size_t bytes, int* status) {
   return q;
 }
 
+ProfScope::ProfScope(hp_plan* plan, const char* name, cudaStream_t stream) : p(plan), s(stream) {
+  ++p->launches;
+  if (!p->prof_on) return;
+  for (size_t i = 0; i < p->prof.size(); ++i)
+    if (p->prof[i].name == name) { idx = (int)i; break; }
+  if (idx < 0) {
+    p->prof.push_back(ProfEntry{});
+    p->prof.back().name = name;
+    idx = (int)p->prof.size() - 1;
+  }
+  if (cudaEventCreate(&a) != cudaSuccess) { cudaGetLastError(); a = nullptr; return; }
+  cudaEventRecord(a, s);
+}
+
+ProfScope::~ProfScope() {
+  if (!a) return;
+  cudaEvent_t b = nullptr;
+  if (cudaEventCreate(&b) != cudaSuccess) { cudaGetLastError(); cudaEventDestroy(a); return; }
+  cudaEventRecord(b, s);
+  p->prof[idx].pending.push_back({a, b});
+}
+
+static void prof_collect(hp_plan* p) {
+  for (auto& e : p->prof) {
+    for (auto& ab : e.pending) {
+      float ms = 0.f;
+      cudaEventSynchronize(ab.second);
+      if (cudaEventElapsedTime(&ms, ab.first, ab.second) == cudaSuccess) { e.ms += ms; e.count += 1; }
+      else cudaGetLastError();
+      cudaEventDestroy(ab.first);
+      cudaEventDestroy(ab.second);
+    }
+    e.pending.clear();
+  }
+}
+
+extern "C" int hp_plan_profile(hp_plan* p, int enable) {
+  if (!p) { hp_set_error("null plan"); return HP_ERR_INVALID; }
+  prof_collect(p);
+  p->prof.clear();
+  p->prof_on = enable != 0;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_profile_get(hp_plan* p, int i, char* name, int name_cap, double* total_ms,
+                                   long long* count) {
+  if (!p || i < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  prof_collect(p);
+  if (i >= (int)p->prof.size()) return HP_ERR_INVALID;
+  const ProfEntry& e = p->prof[i];
+  if (name && name_cap > 0) {
+    std::strncpy(name, e.name.c_str(), name_cap - 1);
+    name[name_cap - 1] = 0;
+  }
+  if (total_ms) *total_ms = e.ms;
+  if (count) *count = e.count;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_launch_count(hp_plan* p, long long* count) {
+  if (!p || !count) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  *count = p->launches;
+  return HP_OK;
+}
+
 static bool valid_N(int N) {
   return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 32;
 }
@@ -90,6 +155,8 @@ extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
   cudaFree(p->rows); cudaFree(p->seg); cudaFree(p->wig64); cudaFree(p->wig32); cudaFree(p->wfull);
   cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_row); cudaFree(p->tap_w);
+  p->prof_on = false;
+  prof_collect(p);
   for (auto& kv : p->ws) cudaFree(kv.second.p);
   delete p;
   return HP_OK;
@@ -213,6 +280,7 @@ extern "C" int hp_fftSO3R_forward(hp_plan* p, const double* f, double* F, int me
   if (p->precision == HP_MIXED) {
     float* t = (float*)p->ws_get("api.f32", sizeof(float) * ng, &st);
     if (st) return st;
+    ProfScope _ps(p, "convert", p->stream);
     k_d2f<<<(unsigned)((ng + 255) / 256), 256, 0, p->stream>>>(df, t, ng);
     HP_CUDA_TRY(cudaGetLastError());
     src = t;
@@ -245,6 +313,7 @@ extern "C" int hp_fftSO3R_backward(hp_plan* p, const double* F, double* f, int m
     float* t = (float*)p->ws_get("api.f32", sizeof(float) * ng, &st);
     if (st) return st;
     HP_CHECK(hp_backward_internal(p, Fi, t, cplx, p->stream));
+    ProfScope _ps(p, "convert", p->stream);
     k_f2d<<<(unsigned)((ng + 255) / 256), 256, 0, p->stream>>>(t, df, ng);
     HP_CUDA_TRY(cudaGetLastError());
   } else {

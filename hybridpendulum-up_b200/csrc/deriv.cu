@@ -353,30 +353,34 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   const RowLayout L = p->layout();
   if (p->ndim == 3) {
     const long long nt = p->nrows * (long long)N * N;
+    ProfScope _ps(p, "deriv.axis3", s);
     k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L);
     HP_CUDA_TRY(cudaGetLastError());
   }
   {
     dim3 grid((unsigned)((p->nx + 127) / 128), (unsigned)p->nm);
+    ProfScope _ps(p, "deriv.local", s);
     k_local<T><<<grid, 128, 0, s>>>(L, Fev, G, p->tap_row, p->tap_w, prm);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  // tiles
+  // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
   constexpr int CT = PlaneCfg<T>::C;
-  static thread_local std::vector<PlaneTile> htiles;
-  htiles.clear();
+  const char* tkey = CT == 2 ? "deriv.tiles2" : "deriv.tiles4";
+  bool have = false;
+  for (auto& kv : p->ws) if (kv.first == tkey) have = true;
+  std::vector<PlaneTile> htiles;
   for (int m = p->m_lo; m <= p->lmax; ++m)
     for (int l = std::abs(m); l <= p->lmax; ++l)
       for (int n0 = -l; n0 <= l; n0 += CT) htiles.push_back({m, l, n0, std::min(CT, l - n0 + 1)});
-  PlaneTile* dt = (PlaneTile*)p->ws_get(CT == 2 ? "deriv.tiles2" : "deriv.tiles4",
-                                        sizeof(PlaneTile) * htiles.size(), &st);
+  PlaneTile* dt = (PlaneTile*)p->ws_get(tkey, sizeof(PlaneTile) * htiles.size(), &st);
   if (st) return st;
-  HP_CUDA_TRY(cudaMemcpyAsync(dt, htiles.data(), sizeof(PlaneTile) * htiles.size(),
-                              cudaMemcpyHostToDevice, s));
-  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!have) {
+    HP_CUDA_TRY(cudaMemcpy(dt, htiles.data(), sizeof(PlaneTile) * htiles.size(), cudaMemcpyHostToDevice));
+  }
   const bool p3 = p->ndim == 3;
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)htiles.size(), p3 ? N : 1);
+  ProfScope _ps(p, "deriv.plane", s);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_plane<N, T, true><<<grid, 256, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);

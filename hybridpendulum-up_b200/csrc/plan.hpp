@@ -27,6 +27,14 @@ struct Buf {
   size_t bytes = 0;
 };
 
+// Per-kernel-family CUDA-event timing (opt-in) and a launch counter.
+struct ProfEntry {
+  std::string name;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  double ms = 0.0;
+  long long count = 0;
+};
+
 struct hp_plan {
   int B = 0, lmax = 0, Bx = 0, N = 0, ndim = 0, precision = 0, symmetry = 0;
   int m_lo = 0, nm = 0, D = 0;     // D = 2lmax+1
@@ -50,6 +58,11 @@ struct hp_plan {
   hp_model model{};
   int* tap_row = nullptr;    // [row][9]  (-1 = no tap)
   double2* tap_w = nullptr;  // [ndim][row][9]
+
+  // profiling
+  bool prof_on = false;
+  std::vector<ProfEntry> prof;
+  long long launches = 0;
 
   // workspace (grow-only), keyed by name
   std::vector<std::pair<std::string, Buf>> ws;
@@ -79,6 +92,17 @@ struct hp_state {
 inline __host__ __device__ int cg1_index(int lmax, int l1, int dl, int m, int m2) {
   return ((l1 * 3 + (dl + 1)) * (2 * lmax + 3) + (m + lmax + 1)) * 3 + (m2 + 1);
 }
+
+// RAII: counts one launch on plan p and, when profiling is on, brackets it
+// with CUDA events recorded on stream s under the family `name`.
+struct ProfScope {
+  hp_plan* p;
+  int idx = -1;
+  cudaEvent_t a = nullptr;
+  cudaStream_t s;
+  ProfScope(hp_plan* plan, const char* name, cudaStream_t stream);
+  ~ProfScope();
+};
 
 // ---- launchers implemented in the .cu files (return hp_status) ----
 int hp_tables_build(hp_plan* p);

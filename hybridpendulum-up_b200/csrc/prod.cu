@@ -84,6 +84,7 @@ int hp_prod_launch(hp_plan* p, const double2* F, const double2* G, double2* FG, 
     HP_CUDA_TRY(cudaGetLastError());
   }
   const long long nt = (long long)D * D * B * batch;
+  ProfScope _ps(p, "prod", s);
   k_prod<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(B, cgt, F, G, FG, batch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;

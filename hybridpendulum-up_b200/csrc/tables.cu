@@ -218,6 +218,7 @@ int hp_full_to_internal(hp_plan* p, const double2* Ff, double2* Fi, cudaStream_t
   const int D = p->D;
   const long long Dfull = (long long)D * D * (p->lmax + 1);
   dim3 grid((unsigned)((Dfull + 31) / 32), (unsigned)((p->nx + 31) / 32));
+  ProfScope _ps(p, "layout", s);
   k_full_to_int<<<grid, dim3(32, 8), 0, s>>>(p->layout(), Ff, Fi);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -227,6 +228,7 @@ int hp_internal_to_full(hp_plan* p, const double2* Fi, double2* Ff, cudaStream_t
   const int D = p->D;
   const long long Dfull = (long long)D * D * (p->lmax + 1);
   dim3 grid((unsigned)((Dfull + 31) / 32), (unsigned)((p->nx + 31) / 32));
+  ProfScope _ps(p, "layout", s);
   k_int_to_full<<<grid, dim3(32, 8), 0, s>>>(p->layout(), Fi, Ff);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;

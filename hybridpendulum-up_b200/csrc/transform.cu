@@ -89,6 +89,12 @@ __global__ void k_transpose(const c2<Tin>* __restrict__ in, c2<Tout>* __restrict
   }
 }
 
+template <typename T>
+__global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = cvt<double2, c2<T>>(in[i]);
+}
+
 // ------------------------------------------------------------ synthesis ----
 // Block = (group of NB consecutive beta indices, range of omega points);
 // the d values of its betas stay in shared memory.  P omega points per batch.
@@ -328,13 +334,18 @@ static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaSt
   const long long nplanes = p->nrows * (p->ndim == 3 ? N : 1);
   if (p->ndim == 3) {
     // plane pass (k1,k2) then line pass along k3, scale applied in the line pass
+    {
+    ProfScope _ps(p, "tf.wplane", s);
     if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
     else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
+    }
     HP_CUDA_TRY(cudaGetLastError());
     const long long nt = p->nrows * (long long)N * N;
+    ProfScope _ps(p, "tf.wline", s);
     if (inv) k_wline<N, T, true><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
     else k_wline<N, T, false><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
   } else {
+    ProfScope _ps(p, "tf.wplane", s);
     if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
     else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
   }
@@ -384,6 +395,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   wblocks = (p->nx + wpb - 1) / wpb;
   HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)wblocks, (unsigned)ngroups);
+  ProfScope _ps(p, "tf.synth", s);
   k_synth<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), Fp,
                                                        p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
                                                                                : (const T*)(const void*)p->wig32,
@@ -416,6 +428,7 @@ static int anal_launch(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
   HP_CUDA_TRY(cudaFuncSetAttribute(k_anal<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)wblocks, (unsigned)ngroups);
   HP_CUDA_TRY(cudaMemsetAsync(Fa, 0, sizeof(C) * p->nrows * p->nx, s));
+  ProfScope _ps(p, "tf.anal", s);
   k_anal<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), f,
                                                       p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
                                                                               : (const T*)(const void*)p->wig32,
@@ -462,7 +475,8 @@ static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out,
   st = omega_fft_any<double, T>(p, Fint, t1, true, s);
   if (st) return st;
   dim3 grid((unsigned)((p->nx + 31) / 32), (unsigned)((p->nrows + 31) / 32));
-  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nrows, p->nx);
+  { ProfScope _ps(p, "tf.transpose", s);
+  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nrows, p->nx); }
   HP_CUDA_TRY(cudaGetLastError());
   if (complex_out) return synth_any<T, true>(p, t2, f, s);
   return synth_any<T, false>(p, t2, f, s);
@@ -480,16 +494,15 @@ static int forward_T(hp_plan* p, const void* f, int complex_in, double2* Fint, c
   st = complex_in ? anal_any<T, true>(p, f, t1, s) : anal_any<T, false>(p, f, t1, s);
   if (st) return st;
   dim3 grid((unsigned)((p->nrows + 31) / 32), (unsigned)((p->nx + 31) / 32));
-  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nx, p->nrows);
+  { ProfScope _ps(p, "tf.transpose", s);
+  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nx, p->nrows); }
   HP_CUDA_TRY(cudaGetLastError());
   st = omega_fft_any<T, T>(p, t2, t1, false, s);
   if (st) return st;
   // to FP64 rows
   const long long n = p->nrows * p->nx;
-  dim3 g2((unsigned)((n + 31) / 32), 1);
-  // reuse the transpose kernel as a converter (1 x n matrix)
-  dim3 gridc((unsigned)((n + 31) / 32), 1);
-  k_transpose<T, double><<<gridc, dim3(32, 8), 0, s>>>(t1, Fint, 1, n);
+  ProfScope _ps(p, "convert", s);
+  k_to_c64<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(t1, Fint, n);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }

@@ -90,6 +90,18 @@ int hp_plan_get_info(const hp_plan* plan, hp_plan_info_t* info);
 int hp_plan_set_stream(hp_plan* plan, void* cuda_stream);
 const char* hp_last_error(void);
 
+/* Measurement hooks (no counterpart in the reference, whose only timing is
+ * tic/toc around each loop step, pendulum.m:270,314).  hp_plan_profile(1)
+ * starts bracketing every kernel launch of the plan with CUDA events on the
+ * plan's stream, grouped by kernel family; hp_plan_profile_get(i, ...) returns
+ * family i's name, summed device time and launch count (HP_ERR_INVALID past
+ * the last family).  hp_plan_launch_count counts every kernel launched by the
+ * plan since creation. */
+int hp_plan_profile(hp_plan* plan, int enable);
+int hp_plan_profile_get(hp_plan* plan, int i, char* name, int name_cap, double* total_ms,
+                        long long* count);
+int hp_plan_launch_count(hp_plan* plan, long long* count);
+
 /* Model for the propagation entry points.  MR: complex (2lmax+1,2lmax+1,lmax+1,ndim)
  * in the full layout; only its degree-1, m2=0 block may be non-zero (the
  * gravity term of pendulum.m:166-192 depends on R through R^T e3 only);

@@ -23,6 +23,7 @@ import math
 from dataclasses import dataclass, field
 
 import numpy as np
+import scipy.fft as sfft
 
 from . import so3
 
@@ -63,7 +64,7 @@ def omega_grid(Bx: int, L: float, ndim: int) -> np.ndarray:
 
 def make_X(x: np.ndarray) -> np.ndarray:
     """X(..., i) = fftn(x_i) (pendulum.m:141-143)."""
-    return np.stack([np.fft.fftn(x[i]) for i in range(x.shape[0])], -1)
+    return np.stack([sfft.fftn(x[i]) for i in range(x.shape[0])], -1)
 
 
 def make_OJO(x: np.ndarray, J: np.ndarray) -> np.ndarray:
@@ -71,7 +72,7 @@ def make_OJO(x: np.ndarray, J: np.ndarray) -> np.ndarray:
     xv = np.moveaxis(x, 0, -1)                      # (..., 3)
     ojo = -np.cross(xv, xv @ J.T)
     ojo = ojo @ np.linalg.inv(J).T
-    return np.stack([np.fft.fftn(ojo[..., i]) for i in range(3)], -1)
+    return np.stack([sfft.fftn(ojo[..., i]) for i in range(3)], -1)
 
 
 def gravity_samples(B: int, mR_matrix: np.ndarray) -> np.ndarray:
@@ -345,10 +346,10 @@ def derivative_fast(F: np.ndarray, P: Pendulum, *, gravity: str = 'l2=1') -> np.
     N = 2 * Bx
     ax = _xaxes(nd)
     u = so3.getu(lmax)
-    Fp = np.fft.ifftn(F, axes=ax)
-    xs = [np.fft.ifftn(P.X[..., i]) for i in range(nd)]          # grid coordinates
+    Fp = sfft.ifftn(F, axes=ax)
+    xs = [sfft.ifftn(P.X[..., i]) for i in range(nd)]          # grid coordinates
     dF = np.zeros_like(F)
-    PF = [np.fft.fftn(Fp * xs[i], axes=ax) for i in range(nd)]   # F_omega[x_i f]
+    PF = [sfft.fftn(Fp * xs[i], axes=ax) for i in range(nd)]   # F_omega[x_i f]
     for l in range(lmax + 1):
         s = slice(lmax - l, lmax + l + 1)
         for i in range(nd):
@@ -365,8 +366,8 @@ def derivative_fast(F: np.ndarray, P: Pendulum, *, gravity: str = 'l2=1') -> np.
         dF -= cmul(-P.b[i] * PF[i], i)
     if nd == 3 and P.OJO is not None:
         for i in range(3):
-            ojo = np.fft.ifftn(P.OJO[..., i])
-            dF -= cmul(np.fft.fftn(Fp * ojo, axes=ax), i)
+            ojo = sfft.ifftn(P.OJO[..., i])
+            dF -= cmul(sfft.fftn(Fp * ojo, axes=ax), i)
     for i in range(nd):
         g = _gravity_literal(F, P.MR[..., i]) if gravity == 'full' else gravity_fast(F, P.MR[..., i])
         dF -= cmul(g, i)

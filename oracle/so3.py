@@ -26,6 +26,7 @@ import math
 from functools import lru_cache
 
 import numpy as np
+import scipy.fft as sfft
 
 
 # ---------------------------------------------------------------- grids ----
@@ -242,8 +243,8 @@ def fftSO3R_forward(f: np.ndarray, B: int | None = None) -> np.ndarray:
     lmax = B - 1
     d, w = wigner_d_table(B), quad_weights(B)
     axes = (0, 2) + tuple(range(3, f.ndim))
-    F1 = np.fft.fftn(f, axes=axes)
-    F1 = np.fft.fftshift(F1, axes=(0, 2))
+    F1 = sfft.fftn(f, axes=axes)
+    F1 = sfft.fftshift(F1, axes=(0, 2))
     F1 = np.flip(F1, axis=(0, 2))
     xs = f.shape[3:]
     F = np.zeros((2 * lmax + 1, 2 * lmax + 1, lmax + 1) + xs, dtype=np.complex128)
@@ -271,10 +272,10 @@ def ifftSO3R_backward(F: np.ndarray, real: bool = True) -> np.ndarray:
     # sum over l of (2l+1) F d, vectorised: entries with l < max(|m|,|n|) are 0 in F and d
     F1[:2 * lmax + 1, :, :2 * lmax + 1] = np.einsum(
         'mnl,mnl...,mnlk->mkn...', np.broadcast_to(l2p1, F.shape[:3]), F, d)
-    F1 = np.fft.ifftshift(F1, axes=(0, 2))
+    F1 = sfft.ifftshift(F1, axes=(0, 2))
     F1 = np.flip(F1, axis=(0, 2))
     axes = (0, 2) + tuple(range(3, F1.ndim))
-    f = np.fft.ifftn(F1, axes=axes) * N ** 2
+    f = sfft.ifftn(F1, axes=axes) * N ** 2
     return f.real if real else f
 
 
