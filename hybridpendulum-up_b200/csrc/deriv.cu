@@ -423,3 +423,128 @@ int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double
   if (p->precision == HP_FP64) return run_deriv<double>(p, Fev, F0, a, out, acc, bacc, s, prm);
   return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm);
 }
+
+// ------------------------------------------ derivative without allocation ----
+// Scratch of hp_pendulum_derivative_noalloc: a file-scope device array that every
+// GPU loading the library holds until exit.  Holds, 256-byte aligned: the
+// coefficients and the derivative in the internal layout, the two intermediate
+// fields of the derivative (P3 = M_3 F and gravity + diffusion), and the plane
+// tile list.  All of it is fully overwritten by each call, so nothing is cleared.
+static constexpr size_t kNoAllocScratchBytes = (size_t)HP_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Address of the scratch array on each device, looked up once per device.
+static void* g_noalloc_addr[64] = {nullptr};
+
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { hp_set_error("device index out of range"); return HP_ERR_INVALID; }
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      hp_set_error(e != cudaSuccess ? cudaGetErrorString(e) : "scratch symbol has no device address");
+      return HP_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = ptr;
+  }
+  *out = g_noalloc_addr[dev];
+  return HP_OK;
+}
+
+// Writes the plane-pass tile list (every (m, l) row cut into chunks of CT
+// consecutive n) on the device, so no host buffer is needed.
+__global__ void k_make_tiles(int m_lo, int lmax, int CT, PlaneTile* tiles) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int k = 0;
+  for (int m = m_lo; m <= lmax; ++m)
+    for (int l = abs(m); l <= lmax; ++l)
+      for (int n0 = -l; n0 <= l; n0 += CT) tiles[k++] = PlaneTile{m, l, n0, min(CT, l - n0 + 1)};
+}
+
+static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+template <int N, typename T>
+static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned char* base,
+                     const DerivParams& prm) {
+  using C = c2<T>;
+  constexpr int CT = PlaneCfg<T>::C;
+  cudaStream_t s = p->stream;
+  const size_t pts = (size_t)p->nrows * p->nx;
+  int ntiles = 0;
+  for (int m = p->m_lo; m <= p->lmax; ++m)
+    for (int l = std::abs(m); l <= p->lmax; ++l) ntiles += (2 * l + 1 + CT - 1) / CT;
+  const bool p3 = p->ndim == 3;
+  size_t off = 0;
+  double2* Fi = reinterpret_cast<double2*>(base + off); off = align256(off + 16 * pts);
+  double2* dFi = reinterpret_cast<double2*>(base + off); off = align256(off + 16 * pts);
+  C* P3 = p3 ? reinterpret_cast<C*>(base + off) : nullptr; if (p3) off = align256(off + sizeof(C) * pts);
+  C* G = reinterpret_cast<C*>(base + off); off = align256(off + sizeof(C) * pts);
+  PlaneTile* tiles = reinterpret_cast<PlaneTile*>(base + off); off = align256(off + sizeof(PlaneTile) * ntiles);
+  if (off > kNoAllocScratchBytes) {
+    hp_set_error("problem too large for the fixed scratch of hp_pendulum_derivative_noalloc "
+                 "(see HP_NOALLOC_SCRATCH_BYTES)");
+    return HP_ERR_SHAPE;
+  }
+  const RowLayout L = p->layout();
+  int st = hp_full_to_internal(p, Ffull, Fi, s);
+  if (st) return st;
+  k_make_tiles<<<1, 1, 0, s>>>(p->m_lo, p->lmax, CT, tiles);
+  HP_CUDA_TRY(cudaGetLastError());
+  if (p3) {
+    const long long nt = p->nrows * (long long)N * N;
+    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fi, P3, (T)prm.L);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  k_local<T><<<dim3((unsigned)((p->nx + 127) / 128), (unsigned)p->nm), 128, 0, s>>>(L, Fi, G, p->tap_row,
+                                                                                   p->tap_w, prm);
+  HP_CUDA_TRY(cudaGetLastError());
+  const size_t smem = plane_smem<T>(N, p3);
+  dim3 grid((unsigned)ntiles, p3 ? N : 1);
+  if (p3) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, true><<<grid, 256, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+  } else {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, false><<<grid, 256, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return hp_internal_to_full(p, dFi, dFfull, s);
+}
+
+template <typename T>
+static int noalloc_T(hp_plan* p, const double2* F, double2* dF, unsigned char* base, const DerivParams& prm) {
+  switch (p->N) {
+    case 4: return noalloc_N<4, T>(p, F, dF, base, prm);
+    case 6: return noalloc_N<6, T>(p, F, dF, base, prm);
+    case 8: return noalloc_N<8, T>(p, F, dF, base, prm);
+    case 12: return noalloc_N<12, T>(p, F, dF, base, prm);
+    case 16: return noalloc_N<16, T>(p, F, dF, base, prm);
+    case 20: return noalloc_N<20, T>(p, F, dF, base, prm);
+    case 24: return noalloc_N<24, T>(p, F, dF, base, prm);
+    case 32: return noalloc_N<32, T>(p, F, dF, base, prm);
+    default:
+      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+extern "C" int hp_pendulum_derivative_noalloc(hp_plan* p, const double* F, double* dF) {
+  if (!p || !F || !dF) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  void* base = nullptr;
+  int st = noalloc_scratch(&base);
+  if (st) return st;
+  DerivParams prm;
+  prm.L = p->model.L;
+  for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; }
+  for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
+  if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
+  const double2* Fin = reinterpret_cast<const double2*>(F);
+  double2* out = reinterpret_cast<double2*>(dF);
+  unsigned char* b = static_cast<unsigned char*>(base);
+  if (p->precision == HP_FP64) return noalloc_T<double>(p, Fin, out, b, prm);
+  return noalloc_T<float>(p, Fin, out, b, prm);
+}

@@ -132,6 +132,25 @@ int hp_pendulum_propagate(hp_plan* plan, const double* Fold, double* Fnew, doubl
 /* The derivative dF of pendulum.m:388-527 / pendulum_reduced.m:362-465. */
 int hp_pendulum_derivative(hp_plan* plan, const double* F, double* dF, int mem);
 
+/* Derivative without allocation: the same dF as hp_pendulum_derivative, for
+ * callers that must not allocate device memory while they run (a propagation
+ * loop on a GPU whose memory another framework owns through its own allocator,
+ * or an estimator working inside a fixed, pre-reserved memory budget), where a
+ * cudaMalloc in the middle of a step can fail, fragment the pool or stall on a
+ * device-wide synchronisation.  No counterpart in the reference.
+ *   F, dF   device pointers, full MATLAB layout (as for hp_pendulum_derivative).
+ * All scratch lives in one static device array of HP_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading the library keeps until the process exits; problems
+ * needing more (FP64: 64 bytes, mixed: 48 bytes per stored coefficient row and
+ * omega point, plus the tile list) return HP_ERR_SHAPE.  The plan and its model
+ * must exist already (hp_plan_create / hp_plan_set_model allocate).  The first
+ * call on a device looks up the array's device address, so make that first call
+ * before any stream capture.  Every call shares the one array: calls that may
+ * overlap on the GPU (other streams, other threads) race and must be ordered by
+ * the caller.  Runs on the plan's stream and returns without synchronising. */
+#define HP_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int hp_pendulum_derivative_noalloc(hp_plan* plan, const double* F, double* dF);
+
 /* Product rule of fftSO3_prod.m:209-265 (complex branch), batched over `batch`
  * independent pairs: FG^l = sum (2l1+1)(2l2+1)/(2l+1) [CG^T (F^l1 kron G^l2) CG]_l.
  * F, G, FG: (2lmax+1, 2lmax+1, lmax+1, batch) complex. */
