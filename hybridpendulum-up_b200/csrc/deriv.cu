@@ -60,21 +60,49 @@ __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __res
 }
 
 // ------------------------------------------------ pass B: gravity + noise ----
-// One thread per omega point, looping over the rows of one m group (taps stay
-// within the group because the gravity multiplier has m2 = 0).
-template <typename T>
-__global__ void __launch_bounds__(128) k_local(RowLayout L, const double2* __restrict__ F,
+// Block = one m group x W consecutive omega points.  The group's rows are
+// staged once in shared memory (taps stay inside the group because the gravity
+// multiplier has m2 = 0); a warp handles one output row at a time, lanes are
+// omega points, so tap metadata is warp-uniform and global accesses coalesced.
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __restrict__ F,
                                                c2<T>* __restrict__ G, const int* __restrict__ tap_row,
                                                const double2* __restrict__ tap_w, DerivParams prm) {
   using C = c2<T>;
-  const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (w >= L.nx) return;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* tile = reinterpret_cast<C*>(smraw);     // [rows of the group][W]
+  const int D = 2 * L.lmax + 1;
+  const int m = (int)blockIdx.y + L.m_lo;
+  const int r0 = L.seg[(m - L.m_lo) * D];
+  const int r1 = (m + 1 <= L.lmax) ? L.seg[(m + 1 - L.m_lo) * D] : (int)L.nrows;
+  const int R = r1 - r0;
+  const long long w0 = (long long)blockIdx.x * W;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // group rows staged with 4 loads in flight per thread
+  for (int e0 = tid; e0 < R * W; e0 += 4 * nth) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * nth;
+      const int r = e / W, w = e % W;
+      v[u] = (e < R * W && w0 + w < L.nx) ? cvt<C, double2>(F[(size_t)(r0 + r) * L.nx + w0 + w]) : czero<C>();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * nth;
+      if (e < R * W) tile[e] = v[u];
+    }
+  }
+  __syncthreads();
+  const int w = tid % W, rl = tid / W, nrl = nth / W;
+  const long long wg = w0 + w;
+  if (wg >= L.nx) return;
   const int N = L.N, nd = L.ndim;
   int kk[3] = {0, 0, 0};
-  long long ww = w;
+  long long ww = wg;
   for (int a = 0; a < nd; ++a) { kk[a] = (int)(ww % N); ww /= N; }
   const double tp = 2.0 * M_PI / prm.L;
-  double d1[3], dd[3];
+  double d1[3] = {0, 0, 0}, dd[3] = {0, 0, 0};
   for (int a = 0; a < nd; ++a) {
     d1[a] = tp * kappa_first(kk[a], N);
     dd[a] = tp * kappa_diag(kk[a], N);
@@ -83,39 +111,37 @@ __global__ void __launch_bounds__(128) k_local(RowLayout L, const double2* __res
   for (int i = 0; i < nd; ++i)
     for (int j = 0; j < nd; ++j)
       noise += (i == j) ? -prm.G[i * 3 + j] * dd[i] * dd[i] : -prm.G[i * 3 + j] * d1[i] * d1[j];
-  // rows of group m = blockIdx.y + m_lo
-  const int D = 2 * L.lmax + 1;
-  const int m = (int)blockIdx.y + L.m_lo;
-  const long long r0 = L.seg[(m - L.m_lo) * D + 0];
-  const long long r1 = (m + 1 <= L.lmax) ? (long long)L.seg[(m + 1 - L.m_lo) * D] : L.nrows;
-  for (long long r = r0; r < r1; ++r) {
-    const double2 f0 = F[r * L.nx + w];
-    double2 acc = make_double2(noise * f0.x, noise * f0.y);
+  for (int r = rl; r < R; r += nrl) {
+    const int rg = r0 + r;
+    const C f0 = tile[r * W + w];
+    double ax = noise * (double)f0.x, ay = noise * (double)f0.y;
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
-      const int src = tap_row[r * 9 + t];
+      const int src = tap_row[rg * 9 + t];
       if (src < 0) continue;
       // coef = -sum_i (i d1_i) W_i
       double cx = 0.0, cy = 0.0;
       for (int i = 0; i < nd; ++i) {
-        const double2 wv = tap_w[((long long)i * L.nrows + r) * 9 + t];
-        cx += d1[i] * wv.y;    // -(i d)(wx + i wy) = d wy - i d wx
+        const double2 wv = tap_w[((size_t)i * L.nrows + rg) * 9 + t];
+        cx += d1[i] * wv.y;
         cy -= d1[i] * wv.x;
       }
-      const double2 fs = F[(long long)src * L.nx + w];
-      acc.x += cx * fs.x - cy * fs.y;
-      acc.y += cx * fs.y + cy * fs.x;
+      const C fs = tile[(src - r0) * W + w];
+      ax += cx * (double)fs.x - cy * (double)fs.y;
+      ay += cx * (double)fs.y + cy * (double)fs.x;
     }
-    G[r * L.nx + w] = cvt<C, double2>(acc);
+    G[(size_t)rg * L.nx + wg] = cvt<C, double2>(make_double2(ax, ay));
   }
 }
+
+template <typename T> static constexpr int local_w() { return sizeof(T) == 8 ? 16 : 32; }
 
 // --------------------------------------------------- pass C: plane pass ----
 struct PlaneTile { int m, l, n0, cnt; };
 
 template <typename T> struct PlaneCfg;
-template <> struct PlaneCfg<double> { static constexpr int C = 2; };
-template <> struct PlaneCfg<float> { static constexpr int C = 4; };
+template <> struct PlaneCfg<double> { static constexpr int C = 1; static constexpr int NT = 128; };
+template <> struct PlaneCfg<float> { static constexpr int C = 2; static constexpr int NT = 256; };
 
 __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, int n) {
   const int am = abs(m), an = abs(n);
@@ -128,7 +154,7 @@ __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, in
 //   [2C+2, 3C+2)       A  = FFT2(Y0) + D_2 FFT2(Y2), then FFT_1
 //   [3C+2, 4C+2)       Y1' = FFT_2(Y1), then D_1 FFT_1
 template <int N, typename T, bool HAS_P3>
-__global__ void __launch_bounds__(256, 1) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
                                                   const double2* __restrict__ Fev,
                                                   const c2<T>* __restrict__ P3,
                                                   const c2<T>* __restrict__ Gl,
@@ -156,22 +182,54 @@ __global__ void __launch_bounds__(256, 1) k_plane(RowLayout L, const PlaneTile* 
   const T inv_n2 = (T)1 / (T)(N * N);
 
   // ---- S1: load F rows n0-1 .. n0+cnt and P3 rows n0 .. n0+cnt-1 ----
+  // Loads are issued in fixed batches of 4 per thread before the shared-memory
+  // stores, so several requests are in flight per thread.
   const int nF = tl.cnt + 2;
-  for (int e = tid; e < nF * N * N; e += nth) {
-    const int s = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
-    const int n = tl.n0 - 1 + s;
-    C v = czero<C>();
-    if (n >= -tl.l && n <= tl.l) {
-      const long long r = row_of(L, tl.l, tl.m, n);
-      v = cvt<C, double2>(Fev[r * L.nx + pbase + q]);
+  {
+    const int tot = nF * N * N;
+    for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        v[u] = czero<C>();
+        if (e < tot) {
+          const int sl = e / (N * N), q = e % (N * N);
+          const int n = tl.n0 - 1 + sl;
+          if (n >= -tl.l && n <= tl.l) v[u] = cvt<C, double2>(Fev[row_of(L, tl.l, tl.m, n) * L.nx + pbase + q]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        if (e < tot) {
+          const int sl = e / (N * N), q = e % (N * N);
+          sF[sl * PS + (q / N) * (N + 1) + q % N] = v[u];
+        }
+      }
     }
-    sF[s * PS + k2 * (N + 1) + k1] = v;
   }
   if (HAS_P3) {
-    for (int e = tid; e < tl.cnt * N * N; e += nth) {
-      const int s = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
-      const long long r = row_of(L, tl.l, tl.m, tl.n0 + s);
-      sP[s * PS + k2 * (N + 1) + k1] = P3[r * L.nx + pbase + q];
+    const int tot = tl.cnt * N * N;
+    for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
+      C v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        v[u] = czero<C>();
+        if (e < tot) {
+          const int sl = e / (N * N), q = e % (N * N);
+          v[u] = P3[row_of(L, tl.l, tl.m, tl.n0 + sl) * L.nx + pbase + q];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        if (e < tot) {
+          const int sl = e / (N * N), q = e % (N * N);
+          sP[sl * PS + (q / N) * (N + 1) + q % N] = v[u];
+        }
+      }
     }
   }
   __syncthreads();
@@ -358,9 +416,12 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
     HP_CUDA_TRY(cudaGetLastError());
   }
   {
-    dim3 grid((unsigned)((p->nx + 127) / 128), (unsigned)p->nm);
+    constexpr int W = local_w<T>();
+    const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
     ProfScope _ps(p, "deriv.local", s);
-    k_local<T><<<grid, 128, 0, s>>>(L, Fev, G, p->tap_row, p->tap_w, prm);
+    k_local<T, W><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_w, prm);
     HP_CUDA_TRY(cudaGetLastError());
   }
   // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
@@ -383,10 +444,10 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   ProfScope _ps(p, "deriv.plane", s);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, 256, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, 256, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -497,17 +558,22 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
     k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fi, P3, (T)prm.L);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  k_local<T><<<dim3((unsigned)((p->nx + 127) / 128), (unsigned)p->nm), 128, 0, s>>>(L, Fi, G, p->tap_row,
-                                                                                   p->tap_w, prm);
+  {
+    constexpr int W = local_w<T>();
+    const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_local<T, W><<<dim3((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm), 256, lsm, s>>>(
+        L, Fi, G, p->tap_row, p->tap_w, prm);
+  }
   HP_CUDA_TRY(cudaGetLastError());
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)ntiles, p3 ? N : 1);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, 256, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, 256, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return hp_internal_to_full(p, dFi, dFfull, s);

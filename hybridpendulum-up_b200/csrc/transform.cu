@@ -19,6 +19,8 @@
 using namespace hp;
 
 // ------------------------------------------------------------ omega FFTs ----
+static int smem_limit();
+
 // 2-D FFT over (k1, k2) of every (row, k3) plane; one block per (row, k3).
 template <int N, typename Tin, typename T, bool INV>
 __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, c2<T>* __restrict__ out,
@@ -28,8 +30,19 @@ __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, 
   const long long pl = blockIdx.x;
   if (pl >= nplanes) return;
   const c2<Tin>* src = in + pl * N * N;
-  for (int e = threadIdx.x; e < N * N; e += blockDim.x)
-    sm[(e / N) * (N + 1) + e % N] = cvt<C, c2<Tin>>(src[e]);
+  for (int e0 = threadIdx.x; e0 < N * N; e0 += 4 * blockDim.x) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      v[u] = e < N * N ? cvt<C, c2<Tin>>(src[e]) : czero<C>();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < N * N) sm[(e / N) * (N + 1) + e % N] = v[u];
+    }
+  }
   __syncthreads();
   for (int k2 = threadIdx.x; k2 < N; k2 += blockDim.x) {
     C x[N];
@@ -96,124 +109,128 @@ __global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out
 }
 
 // ------------------------------------------------------------ synthesis ----
-// Block = (group of NB consecutive beta indices, range of omega points);
-// the d values of its betas stay in shared memory.  P omega points per batch.
-template <int B, typename T, int NB, bool CPLX>
-__global__ void __launch_bounds__(512) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
-                                               const T* __restrict__ wig, void* __restrict__ fout,
-                                               int P, long long w_per_block) {
+// Block = (group of NB consecutive beta indices, range of omega points), the
+// (2l+1)-weighted d values of its betas resident in shared memory.  Input rows
+// are read in the [row][omega] layout with the P omega points of a batch on
+// consecutive lanes, so every coefficient load is coalesced; the per-(omega,
+// beta) intermediates G -> H live in shared memory as [bb][m][q][p].
+template <int B, typename T, int NB, int P, bool CPLX>
+__global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
+                                                  const T* __restrict__ wig, void* __restrict__ fout,
+                                                  int nbatch) {
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
-  constexpr int NM = CPLX ? D : B;          // stored m values
+  constexpr int NM = CPLX ? D : B;
   constexpr int MLO = CPLX ? -lmax : 0;
+  constexpr int NPAIR = NM * D;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* sd = reinterpret_cast<T*>(smraw);                       // [NB][nrows]
-  size_t off = ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
-  C* sG = reinterpret_cast<C*>(smraw + off);                 // [P][NB][NM][NB2]
+  const int nrows = (int)L.nrows;
+  T* sd = reinterpret_cast<T*>(smraw);
+  C* sG = reinterpret_cast<C*>(smraw + ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16);
   const int b0 = blockIdx.y * NB;
+  const int nbv = min(NB, NB2 - b0);
   const int tid = threadIdx.x, nth = blockDim.x;
-  for (long long e = tid; e < (long long)NB * L.nrows; e += nth) {
-    const int bb = (int)(e / L.nrows);
-    sd[e] = (b0 + bb < NB2) ? wig[(long long)(b0 + bb) * L.nrows + e % L.nrows] : (T)0;
+  for (int e = tid; e < NB * nrows; e += nth) {
+    const int bb = e / nrows, r = e % nrows;
+    const T l2 = (T)(2 * L.rows[r].x + 1);
+    sd[e] = (bb < nbv) ? l2 * wig[(size_t)(b0 + bb) * nrows + r] : (T)0;
   }
-  const long long wbeg = blockIdx.x * w_per_block;
-  const long long wend = min(wbeg + w_per_block, L.nx);
-  const int npairs = NM * D;
-  for (long long w0 = wbeg; w0 < wend; w0 += P) {
-    const int pc = (int)min((long long)P, wend - w0);
+  const long long nx = L.nx;
+  for (int bt = 0; bt < nbatch; ++bt) {
+    const long long w0 = ((long long)blockIdx.x * nbatch + bt) * P;
+    if (w0 >= nx) break;
     __syncthreads();
-    // beta stage
-    for (int it = tid; it < pc * npairs; it += nth) {
-      const int p = it / npairs, pr = it % npairs;
+    // beta stage: item (pair, p), p fastest
+    for (int it = tid; it < NPAIR * P; it += nth) {
+      const int p = it % P, pr = it / P;
       const int mi = pr / D, n = pr % D - lmax, m = mi + MLO;
       const int am = abs(m), an = abs(n), lmin = am > an ? am : an;
       const int q = n >= 0 ? n : n + NB2;
-      C* g = sG + ((size_t)p * NB * NM + mi) * NB2;
-      if (n == 0)
-        for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + B] = czero<C>();
-      if (lmin > lmax) {
-        for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + q] = czero<C>();
-        continue;
-      }
-      const long long s = L.seg[(m - L.m_lo) * D + n + lmax];
       C acc[NB];
 #pragma unroll
       for (int bb = 0; bb < NB; ++bb) acc[bb] = czero<C>();
-      const C* src = Fp + (w0 + p) * L.nrows + s;
-      for (int j = 0; j <= lmax - lmin; ++j) {
-        const C v = src[j];
-        const T l2 = (T)(2 * (lmin + j) + 1);
+      if (w0 + p < nx) {
+        const int s = L.seg[(m - L.m_lo) * D + n + lmax];
+        const C* src = Fp + (size_t)s * nx + w0 + p;
+        const T* dsrc = sd + s;
+        const int cnt = lmax - lmin;
+        // all loads of the segment issued before the FMAs (predicated, fully unrolled)
+        C v[B];
 #pragma unroll
-        for (int bb = 0; bb < NB; ++bb) {
-          const T dv = l2 * sd[(size_t)bb * L.nrows + s + j];
-          acc[bb].x += dv * v.x;
-          acc[bb].y += dv * v.y;
+        for (int j = 0; j < B; ++j) v[j] = (j <= cnt) ? src[(size_t)j * nx] : czero<C>();
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+          if (j > cnt) break;
+#pragma unroll
+          for (int bb = 0; bb < NB; ++bb) {
+            const T dv = dsrc[bb * nrows + j];
+            acc[bb].x = fma(dv, v[j].x, acc[bb].x);
+            acc[bb].y = fma(dv, v[j].y, acc[bb].y);
+          }
         }
       }
 #pragma unroll
-      for (int bb = 0; bb < NB; ++bb) g[(size_t)bb * NM * NB2 + q] = acc[bb];
+      for (int bb = 0; bb < NB; ++bb) {
+        C* g = sG + ((bb * NM + mi) * NB2) * P + p;
+        g[q * P] = acc[bb];
+        if (n == 0) g[B * P] = czero<C>();
+      }
     }
     __syncthreads();
-    // gamma stage: rows (p, bb, mi) over n -> c
-    for (int it = tid; it < pc * NB * NM; it += nth) {
-      C* g = sG + (size_t)it * NB2;
+    // gamma stage: item (bb, mi, p): FFT over n -> c, in place
+    for (int it = tid; it < NB * NM * P; it += nth) {
+      C* g = sG + (it / P) * NB2 * P + it % P;
       C x[NB2];
 #pragma unroll
-      for (int j = 0; j < NB2; ++j) x[j] = g[j];
+      for (int j = 0; j < NB2; ++j) x[j] = g[j * P];
       fft<NB2, false>(x);
 #pragma unroll
-      for (int j = 0; j < NB2; ++j) g[j] = x[j];
+      for (int j = 0; j < NB2; ++j) g[j * P] = x[j];
     }
     __syncthreads();
-    // alpha stage: (p, bb, c) over m -> a ; single round (host guarantees pc*NB*NB2 <= nth)
-    const int nalpha = pc * NB * NB2;
-    const bool act = tid < nalpha;
+    // alpha stage: item (bb, c, p), one round (NB * NB2 * P <= blockDim)
+    const bool act = tid < NB * NB2 * P;
+    const int p = tid % P, c = (tid / P) % NB2, bb = tid / (P * NB2);
     C x[NB2];
-    int p = 0, bb = 0, c = 0;
     if (act) {
-      p = tid / (NB * NB2);
-      bb = (tid / NB2) % NB;
-      c = tid % NB2;
-      const C* h = sG + ((size_t)(p * NB + bb) * NM) * NB2 + c;
+      const C* h = sG + (bb * NM * NB2 + c) * P + p;
 #pragma unroll
       for (int q = 0; q < NB2; ++q) x[q] = czero<C>();
       if (CPLX) {
 #pragma unroll
         for (int mi = 0; mi < NM; ++mi) {
           const int m = mi + MLO;
-          x[m >= 0 ? m : m + NB2] = h[(size_t)mi * NB2];
+          x[m >= 0 ? m : m + NB2] = h[mi * NB2 * P];
         }
       } else {
+        x[0] = h[0];
 #pragma unroll
-        for (int m = 0; m < NM; ++m) x[m] = (m == 0 ? (T)1 : (T)2) * h[(size_t)m * NB2];
+        for (int m = 1; m < NM; ++m) x[m] = (T)2 * h[m * NB2 * P];
       }
       fft<NB2, false>(x);
     }
     __syncthreads();
-    if (act) {
-      // stage into sG as [p][c][bb][a]
+    if (act) {  // staging [p][c][bb][a], aliasing sG
       if (CPLX) {
-        C* st = sG + (((size_t)p * NB2 + c) * NB + bb) * NB2;
+        C* st = sG + ((p * NB2 + c) * NB + bb) * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
       } else {
-        T* st = reinterpret_cast<T*>(sG) + (((size_t)p * NB2 + c) * NB + bb) * NB2;
+        T* st = reinterpret_cast<T*>(sG) + ((p * NB2 + c) * NB + bb) * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a].x;
       }
     }
     __syncthreads();
-    // coalesced store: f[a + 2B (b + 2B (c + 2B w))]
-    const int nbv = min(NB, NB2 - b0);
-    const long long per_w = (long long)NB2 * nbv * NB2;
-    for (long long e = tid; e < (long long)pc * per_w; e += nth) {
-      const int pp = (int)(e / per_w);
-      const int r = (int)(e % per_w);
-      const int cc = r / (nbv * NB2), bq = (r / NB2) % nbv, a = r % NB2;
-      const long long gi = (long long)a + NB2 * ((long long)(b0 + bq) + NB2 * ((long long)cc + NB2 * (w0 + pp)));
-      const size_t si = (((size_t)pp * NB2 + cc) * NB + bq) * NB2 + a;
+    // coalesced store: f[a + 2B (b + 2B (c + 2B w))], contiguous nbv*2B run per (w, c)
+    const int run = nbv * NB2;
+    const int pc = (int)min((long long)P, nx - w0);
+    for (int e = tid; e < pc * NB2 * run; e += nth) {
+      const int pp = e / (NB2 * run), r = e % (NB2 * run), cc = r / run, o = r % run;
+      const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2 + o;
+      const int si = ((pp * NB2 + cc) * NB) * NB2 + o;
       if (CPLX) reinterpret_cast<C*>(fout)[gi] = sG[si];
-      else reinterpret_cast<T*>(fout)[gi] = reinterpret_cast<T*>(sG)[si];
+      else reinterpret_cast<T*>(fout)[gi] = reinterpret_cast<const T*>(sG)[si];
     }
   }
 }
@@ -373,33 +390,30 @@ static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cu
 template <int B, typename T, bool CPLX>
 static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   using C = c2<T>;
-  constexpr int NB = TfCfg<T>::NB, NB2 = 2 * B;
+  constexpr int NB = 2, NB2 = 2 * B, P = (256 / (NB * NB2)) > 0 ? 256 / (NB * NB2) : 1;
   constexpr int NM = CPLX ? 2 * B - 1 : B;
-  const int threads = TfCfg<T>::threads;
+  static_assert(NB * NB2 * P <= 256, "alpha stage must fit one round");
   const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
-  const size_t per_p = std::max((size_t)NB * NM * NB2 * sizeof(C),
-                                (size_t)NB * NB2 * NB2 * (CPLX ? sizeof(C) : sizeof(T)));
-  const int lim = smem_limit();
-  int P = std::max(1, threads / (NB * NB2));
-  while (P > 1 && sd_bytes + P * per_p > (size_t)lim) --P;
-  if (sd_bytes + P * per_p > (size_t)lim) {
+  const size_t sg_bytes = std::max((size_t)NB * NM * NB2 * P * sizeof(C),
+                                   (size_t)P * NB2 * NB * NB2 * (CPLX ? sizeof(C) : sizeof(T)));
+  const size_t smem = sd_bytes + sg_bytes;
+  if (smem > (size_t)smem_limit()) {
     hp_set_error("synthesis tables exceed shared memory for this bandlimit");
     return HP_ERR_UNSUPPORTED;
   }
-  const size_t smem = sd_bytes + P * per_p;
   const int ngroups = (NB2 + NB - 1) / NB;
-  // enough blocks to fill the machine several times over
-  long long wblocks = std::max(1LL, std::min(p->nx, 8LL * 148 * 2 / ngroups + 1));
-  long long wpb = (p->nx + wblocks - 1) / wblocks;
-  wpb = (wpb + P - 1) / P * P;
-  wblocks = (p->nx + wpb - 1) / wpb;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)wblocks, (unsigned)ngroups);
+  const long long nbatches = (p->nx + P - 1) / P;
+  // about 8 resident waves of blocks over 148 SMs
+  long long gx = std::max(1LL, (148LL * 2 * 8) / ngroups);
+  int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
+  gx = (nbatches + nbatch - 1) / nbatch;
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((unsigned)gx, (unsigned)ngroups);
   ProfScope _ps(p, "tf.synth", s);
-  k_synth<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), Fp,
-                                                       p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
-                                                                               : (const T*)(const void*)p->wig32,
-                                                       f, P, wpb);
+  k_synth<B, T, NB, P, CPLX><<<grid, 256, smem, s>>>(p->layout(), Fp,
+                                                     p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
+                                                                             : (const T*)(const void*)p->wig32,
+                                                     f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
@@ -470,16 +484,10 @@ static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out,
   const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
   C* t1 = (C*)p->ws_get("tf.t1", fb, &st);
   if (st) return st;
-  C* t2 = (C*)p->ws_get("tf.t2", fb, &st);
-  if (st) return st;
   st = omega_fft_any<double, T>(p, Fint, t1, true, s);
   if (st) return st;
-  dim3 grid((unsigned)((p->nx + 31) / 32), (unsigned)((p->nrows + 31) / 32));
-  { ProfScope _ps(p, "tf.transpose", s);
-  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nrows, p->nx); }
-  HP_CUDA_TRY(cudaGetLastError());
-  if (complex_out) return synth_any<T, true>(p, t2, f, s);
-  return synth_any<T, false>(p, t2, f, s);
+  if (complex_out) return synth_any<T, true>(p, t1, f, s);
+  return synth_any<T, false>(p, t1, f, s);
 }
 
 template <typename T>
