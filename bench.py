@@ -323,7 +323,8 @@ def main():
     # per-kernel device time of the same timed loop, in a second pass with event brackets
     _, _, prof, _ = timed(smix, fmix, pmix, K, 1, profile=True)
     K64 = args.fp64_steps or K
-    ms_64, clocks64, prof64, _ = timed(s64, f64, p64, K64, W, profile=False)
+    ms_64, clocks64, _, _ = timed(s64, f64, p64, K64, W, profile=False)
+    _, _, prof64, _ = timed(s64, f64, p64, K64, 1, profile=True)
 
     # accuracy of the mixed step against the FP64 step from the same state
     ta = hp.State(pmix)
@@ -419,7 +420,8 @@ def main():
                    'step_includes': ['derivative (Lie, damping, gyroscopic, CG gravity, diffusion)',
                                      'Euler update (FP64)', 'inverse omega FFT', 'SO(3) synthesis to f']},
         'fp64': {'value': round(value64, 3), 'ms_per_step': round(ms_64 / K64, 4), 'steps': K64,
-                 'clocks_sm_mhz': clocks64.get('sm_mhz')},
+                 'clocks_sm_mhz': clocks64.get('sm_mhz'),
+                 'kernel_ms_per_launch': {k: round(v[0] / max(v[1], 1), 4) for k, v in prof64.items()}},
         'speedup_mixed_vs_fp64': round(value / value64, 3),
         'accuracy_mixed_vs_fp64': {'step_increment_rel_l2': err_step, 'F_rel_l2': err_F,
                                    'density_rel_l2': err_f, 'density_max_rel': err_fmax,

@@ -154,7 +154,7 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
 extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
   cudaFree(p->rows); cudaFree(p->seg); cudaFree(p->wig64); cudaFree(p->wig32); cudaFree(p->wfull);
-  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_row); cudaFree(p->tap_w);
+  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_row); cudaFree(p->tap_cnt); cudaFree(p->tap_w);
   p->prof_on = false;
   prof_collect(p);
   for (auto& kv : p->ws) cudaFree(kv.second.p);

@@ -102,6 +102,38 @@ __device__ __forceinline__ void dft_small(C (&v)[R]) {
     C t3r;
     if (INV) { t3r.x = -t3.y; t3r.y = t3.x; } else { t3r.x = t3.y; t3r.y = -t3.x; }
     v[0] = t0 + t2; v[2] = t0 - t2; v[1] = t1 + t3r; v[3] = t1 - t3r;
+  } else if constexpr (R == 3) {
+    // y0 = x0 + s, y1,2 = x0 - s/2 -+ i (sqrt3/2) d  (forward), s = x1 + x2, d = x1 - x2
+    using T = decltype(v[0].x);
+    const T h = (T)0.86602540378443864676;  // sin(pi/3)
+    C s = v[1] + v[2], d = v[1] - v[2];
+    C a;
+    a.x = v[0].x - (T)0.5 * s.x;
+    a.y = v[0].y - (T)0.5 * s.y;
+    C t;  // -i h d (forward) or +i h d (inverse)
+    if (INV) { t.x = -h * d.y; t.y = h * d.x; } else { t.x = h * d.y; t.y = -h * d.x; }
+    v[0] = v[0] + s;
+    v[1] = a + t;
+    v[2] = a - t;
+  } else if constexpr (R == 5) {
+    using T = decltype(v[0].x);
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    const C s14 = v[1] + v[4], d14 = v[1] - v[4], s23 = v[2] + v[3], d23 = v[2] - v[3];
+    C a1, a2, b1, b2;
+    a1.x = v[0].x + c1 * s14.x + c2 * s23.x;  a1.y = v[0].y + c1 * s14.y + c2 * s23.y;
+    a2.x = v[0].x + c2 * s14.x + c1 * s23.x;  a2.y = v[0].y + c2 * s14.y + c1 * s23.y;
+    b1.x = s1 * d14.x + s2 * d23.x;            b1.y = s1 * d14.y + s2 * d23.y;
+    b2.x = s2 * d14.x - s1 * d23.x;            b2.y = s2 * d14.y - s1 * d23.y;
+    // forward: y1 = a1 - i b1, y4 = a1 + i b1, y2 = a2 - i b2, y3 = a2 + i b2
+    C ib1, ib2;
+    if (INV) { ib1.x = b1.y; ib1.y = -b1.x; ib2.x = b2.y; ib2.y = -b2.x; }   // -(i b)
+    else { ib1.x = -b1.y; ib1.y = b1.x; ib2.x = -b2.y; ib2.y = b2.x; }      // +(i b)
+    v[0] = v[0] + s14 + s23;
+    v[1] = a1 - ib1;
+    v[4] = a1 + ib1;
+    v[2] = a2 - ib2;
+    v[3] = a2 + ib2;
   } else {
     C o[R];
 #pragma unroll

@@ -64,9 +64,10 @@ __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __res
 // staged once in shared memory (taps stay inside the group because the gravity
 // multiplier has m2 = 0); a warp handles one output row at a time, lanes are
 // omega points, so tap metadata is warp-uniform and global accesses coalesced.
-template <typename T, int W>
+template <typename T, int W, int NDIM>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __restrict__ F,
                                                c2<T>* __restrict__ G, const int* __restrict__ tap_row,
+                                               const int* __restrict__ tap_cnt,
                                                const double2* __restrict__ tap_w, DerivParams prm) {
   using C = c2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -97,40 +98,48 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
   const int w = tid % W, rl = tid / W, nrl = nth / W;
   const long long wg = w0 + w;
   if (wg >= L.nx) return;
-  const int N = L.N, nd = L.ndim;
-  int kk[3] = {0, 0, 0};
-  long long ww = wg;
-  for (int a = 0; a < nd; ++a) { kk[a] = (int)(ww % N); ww /= N; }
-  const double tp = 2.0 * M_PI / prm.L;
-  double d1[3] = {0, 0, 0}, dd[3] = {0, 0, 0};
-  for (int a = 0; a < nd; ++a) {
-    d1[a] = tp * kappa_first(kk[a], N);
-    dd[a] = tp * kappa_diag(kk[a], N);
+  const int N = L.N;
+  const T tp = (T)(2.0 * M_PI / prm.L);
+  T d1[NDIM], dd[NDIM];
+  {
+    long long ww = wg;
+#pragma unroll
+    for (int a = 0; a < NDIM; ++a) {
+      const int k = (int)(ww % N);
+      ww /= N;
+      d1[a] = tp * (T)kappa_first(k, N);
+      dd[a] = tp * (T)kappa_diag(k, N);
+    }
   }
-  double noise = 0.0;
-  for (int i = 0; i < nd; ++i)
-    for (int j = 0; j < nd; ++j)
-      noise += (i == j) ? -prm.G[i * 3 + j] * dd[i] * dd[i] : -prm.G[i * 3 + j] * d1[i] * d1[j];
+  T noise = 0;
+#pragma unroll
+  for (int i = 0; i < NDIM; ++i)
+#pragma unroll
+    for (int j = 0; j < NDIM; ++j)
+      noise -= (T)prm.G[i * 3 + j] * ((i == j) ? dd[i] * dd[i] : d1[i] * d1[j]);
   for (int r = rl; r < R; r += nrl) {
     const int rg = r0 + r;
     const C f0 = tile[r * W + w];
-    double ax = noise * (double)f0.x, ay = noise * (double)f0.y;
-#pragma unroll
-    for (int t = 0; t < 9; ++t) {
+    T ax = noise * f0.x, ay = noise * f0.y;
+    const int cnt = tap_cnt[rg];
+    for (int t = 0; t < cnt; ++t) {
       const int src = tap_row[rg * 9 + t];
-      if (src < 0) continue;
-      // coef = -sum_i (i d1_i) W_i
-      double cx = 0.0, cy = 0.0;
-      for (int i = 0; i < nd; ++i) {
-        const double2 wv = tap_w[((size_t)i * L.nrows + rg) * 9 + t];
-        cx += d1[i] * wv.y;
-        cy -= d1[i] * wv.x;
+      // coef = -sum_i (i d1_i) W_i = sum_i d1_i (W_i.y - i W_i.x)
+      T cx = 0, cy = 0;
+#pragma unroll
+      for (int i = 0; i < NDIM; ++i) {
+        const double2 wv = tap_w[(rg * 9 + t) * 3 + i];
+        cx += d1[i] * (T)wv.y;
+        cy -= d1[i] * (T)wv.x;
       }
       const C fs = tile[(src - r0) * W + w];
-      ax += cx * (double)fs.x - cy * (double)fs.y;
-      ay += cx * (double)fs.y + cy * (double)fs.x;
+      ax += cx * fs.x - cy * fs.y;
+      ay += cx * fs.y + cy * fs.x;
     }
-    G[(size_t)rg * L.nx + wg] = cvt<C, double2>(make_double2(ax, ay));
+    C o;
+    o.x = ax;
+    o.y = ay;
+    G[(size_t)rg * L.nx + wg] = o;
   }
 }
 
@@ -182,15 +191,15 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
   const T inv_n2 = (T)1 / (T)(N * N);
 
   // ---- S1: load F rows n0-1 .. n0+cnt and P3 rows n0 .. n0+cnt-1 ----
-  // Loads are issued in fixed batches of 4 per thread before the shared-memory
+  // Loads are issued in fixed batches of 8 per thread before the shared-memory
   // stores, so several requests are in flight per thread.
   const int nF = tl.cnt + 2;
   {
     const int tot = nF * N * N;
-    for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
-      C v[4];
+    for (int e0 = tid; e0 < tot; e0 += 8 * nth) {
+      C v[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int e = e0 + u * nth;
         v[u] = czero<C>();
         if (e < tot) {
@@ -200,7 +209,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
         }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int e = e0 + u * nth;
         if (e < tot) {
           const int sl = e / (N * N), q = e % (N * N);
@@ -211,10 +220,10 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
   }
   if (HAS_P3) {
     const int tot = tl.cnt * N * N;
-    for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
-      C v[4];
+    for (int e0 = tid; e0 < tot; e0 += 8 * nth) {
+      C v[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int e = e0 + u * nth;
         v[u] = czero<C>();
         if (e < tot) {
@@ -223,7 +232,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
         }
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
+      for (int u = 0; u < 8; ++u) {
         const int e = e0 + u * nth;
         if (e < tot) {
           const int sl = e / (N * N), q = e % (N * N);
@@ -368,22 +377,42 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
   __syncthreads();
 
   // ---- S6: dF = A + Y1' + G ; out = F0 + a dF ; acc += bacc dF ----
-  for (int e = tid; e < tl.cnt * N * N; e += nth) {
-    const int c = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
-    const long long r = row_of(L, tl.l, tl.m, tl.n0 + c);
-    const long long gi = r * L.nx + pbase + q;
-    const C s = sA[c * PS + k2 * (N + 1) + k1] + sY[c * PS + k2 * (N + 1) + k1];
-    const C g = Gl[gi];
-    const double dx = (double)s.x + (double)g.x, dy = (double)s.y + (double)g.y;
-    double2 o = F0 ? F0[gi] : make_double2(0.0, 0.0);
-    o.x += a * dx;
-    o.y += a * dy;
-    out[gi] = o;
-    if (acc) {
-      double2 v = acc[gi];
-      v.x += bacc * dx;
-      v.y += bacc * dy;
-      acc[gi] = v;
+  {
+    const int tot = tl.cnt * N * N;
+    for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
+      C g[4];
+      double2 f0[4], ac[4];
+      long long gi[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        gi[u] = -1;
+        if (e < tot) {
+          const int c = e / (N * N), q = e % (N * N);
+          gi[u] = row_of(L, tl.l, tl.m, tl.n0 + c) * L.nx + pbase + q;
+          g[u] = Gl[gi[u]];
+          f0[u] = F0 ? F0[gi[u]] : make_double2(0.0, 0.0);
+          if (acc) ac[u] = acc[gi[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * nth;
+        if (e >= tot) continue;
+        const int c = e / (N * N), q = e % (N * N), k1 = q % N, k2 = q / N;
+        const C s = sA[c * PS + k2 * (N + 1) + k1] + sY[c * PS + k2 * (N + 1) + k1];
+        const double dx = (double)s.x + (double)g[u].x, dy = (double)s.y + (double)g[u].y;
+        double2 o = f0[u];
+        o.x += a * dx;
+        o.y += a * dy;
+        out[gi[u]] = o;
+        if (acc) {
+          double2 v = ac[u];
+          v.x += bacc * dx;
+          v.y += bacc * dy;
+          acc[gi[u]] = v;
+        }
+      }
     }
   }
 }
@@ -418,10 +447,15 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   {
     constexpr int W = local_w<T>();
     const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
     dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
     ProfScope _ps(p, "deriv.local", s);
-    k_local<T, W><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_w, prm);
+    if (p->ndim == 3) {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+      k_local<T, W, 3><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+    } else {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+      k_local<T, W, 2><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+    }
     HP_CUDA_TRY(cudaGetLastError());
   }
   // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
@@ -561,9 +595,14 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   {
     constexpr int W = local_w<T>();
     const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W><<<dim3((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm), 256, lsm, s>>>(
-        L, Fi, G, p->tap_row, p->tap_w, prm);
+    const dim3 lg((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
+    if (p->ndim == 3) {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+      k_local<T, W, 3><<<lg, 256, lsm, s>>>(L, Fi, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+    } else {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+      k_local<T, W, 2><<<lg, 256, lsm, s>>>(L, Fi, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+    }
   }
   HP_CUDA_TRY(cudaGetLastError());
   const size_t smem = plane_smem<T>(N, p3);

@@ -56,8 +56,9 @@ struct hp_plan {
   // model
   bool has_model = false;
   hp_model model{};
-  int* tap_row = nullptr;    // [row][9]  (-1 = no tap)
-  double2* tap_w = nullptr;  // [ndim][row][9]
+  int* tap_row = nullptr;    // [row][9] source rows of the non-zero taps
+  int* tap_cnt = nullptr;    // [row] number of non-zero taps
+  double2* tap_w = nullptr;  // [row][9][3] weights per component
 
   // profiling
   bool prof_on = false;

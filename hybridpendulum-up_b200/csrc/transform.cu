@@ -130,8 +130,8 @@ __global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __re
   const int b0 = blockIdx.y * NB;
   const int nbv = min(NB, NB2 - b0);
   const int tid = threadIdx.x, nth = blockDim.x;
-  for (int e = tid; e < NB * nrows; e += nth) {
-    const int bb = e / nrows, r = e % nrows;
+  for (int e = tid; e < NB * nrows; e += nth) {   // interleaved [row][bb]
+    const int r = e / NB, bb = e % NB;
     const T l2 = (T)(2 * L.rows[r].x + 1);
     sd[e] = (bb < nbv) ? l2 * wig[(size_t)(b0 + bb) * nrows + r] : (T)0;
   }
@@ -152,20 +152,21 @@ __global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __re
       if (w0 + p < nx) {
         const int s = L.seg[(m - L.m_lo) * D + n + lmax];
         const C* src = Fp + (size_t)s * nx + w0 + p;
-        const T* dsrc = sd + s;
-        const int cnt = lmax - lmin;
-        // all loads of the segment issued before the FMAs (predicated, fully unrolled)
-        C v[B];
+        const T* dsrc = sd + (size_t)s * NB;
+        const int len = lmax - lmin + 1;
+        // loads issued in batches of 4 ahead of their FMAs
+        for (int j0 = 0; j0 < len; j0 += 4) {
+          C v[4];
 #pragma unroll
-        for (int j = 0; j < B; ++j) v[j] = (j <= cnt) ? src[(size_t)j * nx] : czero<C>();
+          for (int u = 0; u < 4; ++u) v[u] = (j0 + u < len) ? src[(size_t)(j0 + u) * nx] : czero<C>();
 #pragma unroll
-        for (int j = 0; j < B; ++j) {
-          if (j > cnt) break;
+          for (int u = 0; u < 4; ++u) {
 #pragma unroll
-          for (int bb = 0; bb < NB; ++bb) {
-            const T dv = dsrc[bb * nrows + j];
-            acc[bb].x = fma(dv, v[j].x, acc[bb].x);
-            acc[bb].y = fma(dv, v[j].y, acc[bb].y);
+            for (int bb = 0; bb < NB; ++bb) {
+              const T dv = (j0 + u < len) ? dsrc[(j0 + u) * NB + bb] : (T)0;
+              acc[bb].x = fma(dv, v[u].x, acc[bb].x);
+              acc[bb].y = fma(dv, v[u].y, acc[bb].y);
+            }
           }
         }
       }
@@ -188,9 +189,13 @@ __global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __re
       for (int j = 0; j < NB2; ++j) g[j * P] = x[j];
     }
     __syncthreads();
-    // alpha stage: item (bb, c, p), one round (NB * NB2 * P <= blockDim)
-    const bool act = tid < NB * NB2 * P;
-    const int p = tid % P, c = (tid / P) % NB2, bb = tid / (P * NB2);
+    // alpha stage, one round (host guarantees the item count fits the block).
+    // Real plans: f_c = Re FFT(w_m H[m][c]) = FFT(h_c) with h_c the Hermitian
+    // extension of H[.][c] (h[0] = Re H[0]); two columns c, c+B share one complex
+    // FFT, FFT(h_c + i h_c') = f_c + i f_c'.  Complex plans: one FFT per column.
+    constexpr int NCOL = CPLX ? NB2 : B;   // FFTs per (bb, p)
+    const bool act = tid < NB * NCOL * P;
+    const int p = tid % P, c = (tid / P) % NCOL, bb = tid / (P * NCOL);
     C x[NB2];
     if (act) {
       const C* h = sG + (bb * NM * NB2 + c) * P + p;
@@ -203,9 +208,21 @@ __global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __re
           x[m >= 0 ? m : m + NB2] = h[mi * NB2 * P];
         }
       } else {
-        x[0] = h[0];
+        const C* h2 = h + B * P;   // column c + B
+        {
+          const C u = h[0], v = h2[0];
+          x[0].x = u.x;
+          x[0].y = v.x;
+        }
 #pragma unroll
-        for (int m = 1; m < NM; ++m) x[m] = (T)2 * h[m * NB2 * P];
+        for (int m = 1; m < B; ++m) {
+          const C u = h[m * NB2 * P], v = h2[m * NB2 * P];
+          // z[m] = u + i v ; z[N-m] = conj(u) + i conj(v)
+          x[m].x = u.x - v.y;
+          x[m].y = u.y + v.x;
+          x[NB2 - m].x = u.x + v.y;
+          x[NB2 - m].y = -u.y + v.x;
+        }
       }
       fft<NB2, false>(x);
     }
@@ -217,20 +234,39 @@ __global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __re
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
       } else {
         T* st = reinterpret_cast<T*>(sG) + ((p * NB2 + c) * NB + bb) * NB2;
+        T* st2 = reinterpret_cast<T*>(sG) + ((p * NB2 + c + B) * NB + bb) * NB2;
 #pragma unroll
-        for (int a = 0; a < NB2; ++a) st[a] = x[a].x;
+        for (int a = 0; a < NB2; ++a) {
+          st[a] = x[a].x;
+          st2[a] = x[a].y;
+        }
       }
     }
     __syncthreads();
-    // coalesced store: f[a + 2B (b + 2B (c + 2B w))], contiguous nbv*2B run per (w, c)
-    const int run = nbv * NB2;
+    // store: f[a + 2B (b + 2B (c + 2B w))]; the nbv*2B values of one (w, c) are
+    // contiguous in f and in the staging buffer, one thread copies one run.
     const int pc = (int)min((long long)P, nx - w0);
-    for (int e = tid; e < pc * NB2 * run; e += nth) {
-      const int pp = e / (NB2 * run), r = e % (NB2 * run), cc = r / run, o = r % run;
-      const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2 + o;
-      const int si = ((pp * NB2 + cc) * NB) * NB2 + o;
-      if (CPLX) reinterpret_cast<C*>(fout)[gi] = sG[si];
-      else reinterpret_cast<T*>(fout)[gi] = reinterpret_cast<const T*>(sG)[si];
+    constexpr int RUN = NB * NB2;
+    for (int e = tid; e < pc * NB2; e += nth) {
+      const int pp = e / NB2, cc = e % NB2;
+      const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2;
+      const int si = (pp * NB2 + cc) * RUN;
+      if (CPLX) {
+        C* dst = reinterpret_cast<C*>(fout) + gi;
+        for (int o = 0; o < nbv * NB2; ++o) dst[o] = sG[si + o];
+      } else {
+        T* dst = reinterpret_cast<T*>(fout) + gi;
+        const T* src = reinterpret_cast<const T*>(sG) + si;
+        constexpr int VW = 16 / sizeof(T);   // elements per 16-byte vector
+        const bool vec = nbv == NB && (RUN % VW) == 0 && ((gi % VW) == 0) && ((si % VW) == 0);
+        if (vec) {
+#pragma unroll
+          for (int o = 0; o < RUN; o += VW)
+            *reinterpret_cast<float4*>(dst + o) = *reinterpret_cast<const float4*>(src + o);
+        } else {
+          for (int o = 0; o < nbv * NB2; ++o) dst[o] = src[o];
+        }
+      }
     }
   }
 }
@@ -387,12 +423,37 @@ static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cu
   }
 }
 
+// (NB, P) of the synthesis: betas per block and omega points per batch, chosen
+// so that shared memory allows two resident blocks where possible and the
+// alpha stage fits one round of 256 threads.
+template <int B, typename T, bool CPLX> struct SynthCfg {
+  static constexpr long long nrows = CPLX ? (long long)B * (2 * B - 1) * (2 * B + 1) / 3
+                                          : (long long)B * (B + 1) * (4 * B - 1) / 6;
+  static constexpr int NM = CPLX ? 2 * B - 1 : B;
+  static constexpr int NCOL = CPLX ? 2 * B : B;
+  static constexpr long long bytes(int nb, int p) {
+    const long long g = (long long)NM * 2 * B * 2 * (long long)sizeof(T);            // G/H, complex
+    const long long st = (long long)2 * B * 2 * B * (CPLX ? 2 : 1) * (long long)sizeof(T);  // f staging
+    return nb * nrows * (long long)sizeof(T) + 16 + (long long)nb * p * (g > st ? g : st);
+  }
+  // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB)
+  static constexpr long long budget() { return bytes(1, 4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
+  static constexpr int pick_nb() { return bytes(2, 4) <= budget() ? 2 : 1; }
+  static constexpr int NB = pick_nb();
+  static constexpr int pick_p() {
+    int p = 8;
+    while (p > 1 && (bytes(NB, p) > budget() || NB * NCOL * p > 256)) p /= 2;
+    return p;
+  }
+  static constexpr int P = pick_p();
+};
+
 template <int B, typename T, bool CPLX>
 static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   using C = c2<T>;
-  constexpr int NB = 2, NB2 = 2 * B, P = (256 / (NB * NB2)) > 0 ? 256 / (NB * NB2) : 1;
-  constexpr int NM = CPLX ? 2 * B - 1 : B;
-  static_assert(NB * NB2 * P <= 256, "alpha stage must fit one round");
+  using Cfg = SynthCfg<B, T, CPLX>;
+  constexpr int NB = Cfg::NB, P = Cfg::P, NB2 = 2 * B, NM = Cfg::NM;
+  static_assert(NB * Cfg::NCOL * P <= 256, "alpha stage must fit one round");
   const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
   const size_t sg_bytes = std::max((size_t)NB * NM * NB2 * P * sizeof(C),
                                    (size_t)P * NB2 * NB * NB2 * (CPLX ? sizeof(C) : sizeof(T)));
