@@ -238,6 +238,27 @@ def cpu_baseline_obj(B, Bx, steps=1):
                       f'(omega-FFT log factor ignored, which favours the CPU)'}
 
 
+# ------------------------------------------------------------ replicas ----
+def replica_seed(rank: int) -> int:
+    """Each rank propagates its own independent density (no data exchange)."""
+    return rank
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Slowest rank's time: the job's time for weak-scaled replicas."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, steps: int, max_ms: float) -> float:
+    """Steps/s of the whole job: every rank did `steps` steps in `max_ms`."""
+    return world * steps / (max_ms / 1e3)
+
+
 # ---------------------------------------------------------------- main ----
 def main():
     args = parse()
@@ -261,7 +282,7 @@ def main():
         torch.distributed.init_process_group('nccl', timeout=datetime.timedelta(seconds=600))
     hp = importlib.import_module('hybridpendulum-up_b200')
     stream = torch.cuda.current_stream(dev)
-    inp = model_inputs(hp, B, Bx, seed=rank)
+    inp = model_inputs(hp, B, Bx, seed=replica_seed(rank))
     L, dt = PARAMS['L'], PARAMS['dt']
 
     def make(prec):
@@ -313,10 +334,7 @@ def main():
         if profile:
             plan.profile(False)
         launches = plan.launch_count() - n0
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item()), clocks, prof, launches
+        return max_over_ranks(ms, world, dev), clocks, prof, launches
 
     K, W = args.steps, max(args.warmup, 3)
     ms_mix, clocks, prof, launches = timed(smix, fmix, pmix, K, W, profile=False)
@@ -349,8 +367,8 @@ def main():
     mass_drift = abs(smix.mass() - mass0) / abs(mass0)
     del ta, tb, Fs, Fa, Fb, dF
 
-    value = world * K / (ms_mix / 1e3)
-    value64 = world * K64 / (ms_64 / 1e3)
+    value = whole_job_rate(world, K, ms_mix)
+    value64 = whole_job_rate(world, K64, ms_64)
 
     # roofline of the dominant kernel family
     peaks, peak_src = load_peaks()
@@ -387,13 +405,10 @@ def main():
             pmix.backward(Fn, out=fh)
             Fh, Fn = Fn, Fh
         barrier()
-        dt_e2e = time.perf_counter() - t0
-        tt = torch.tensor([dt_e2e], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        dt_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
         bi = 2 * Fh.numel() * 16
         bo = Fh.numel() * 16 + fh.numel() * 8
-        e2e = {'value': world * args.e2e_steps / float(tt.item()), 'unit': 'steps/s',
+        e2e = {'value': whole_job_rate(world, args.e2e_steps, dt_e2e * 1e3), 'unit': 'steps/s',
                'h2d_bytes_per_step': bi, 'd2h_bytes_per_step': bo,
                'api': 'hp_pendulum_propagate + hp_fftSO3R_backward, host (pinned) MATLAB-layout buffers'}
 

@@ -115,7 +115,7 @@ __global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out
 // consecutive lanes, so every coefficient load is coalesced; the per-(omega,
 // beta) intermediates G -> H live in shared memory as [bb][m][q][p].
 template <int B, typename T, int NB, int P, bool CPLX>
-__global__ void __launch_bounds__(256, 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
                                                   const T* __restrict__ wig, void* __restrict__ fout,
                                                   int nbatch) {
   using C = c2<T>;

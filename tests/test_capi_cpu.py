@@ -1,0 +1,68 @@
+"""The C ABI without a GPU: the library loads, exports every symbol that
+include/hp.h declares, validates arguments and reports errors; host-side logic
+of the Python mirror (MEX-argument checks) against the oracle."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import pendulum as pd
+from oracle import so3
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    h = open(os.path.join(ROOT, 'include', 'hp.h')).read()
+    return re.findall(r'^\s*(?:int|const char\*)\s+(hp_\w+)\s*\(', h, re.M)
+
+
+def test_every_declared_symbol_is_exported(hp):
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(hp._lib, s), s
+
+
+def test_argument_validation_without_gpu(hp):
+    lib = hp._lib
+    h = ctypes.c_void_p()
+    assert lib.hp_plan_create(ctypes.byref(h), 7, 2, 3, 0, 0) == hp.HP_ERR_INVALID      # B not supported
+    assert b'bandlimit' in lib.hp_last_error()
+    assert lib.hp_plan_create(ctypes.byref(h), 4, 5, 3, 0, 0) == hp.HP_ERR_INVALID      # 2Bx = 10
+    assert lib.hp_plan_create(ctypes.byref(h), 4, 2, 4, 0, 0) == hp.HP_ERR_INVALID      # ndim
+    assert lib.hp_plan_create(ctypes.byref(h), 4, 2, 3, 5, 0) == hp.HP_ERR_INVALID      # precision
+    assert lib.hp_plan_create(None, 4, 2, 3, 0, 0) == hp.HP_ERR_INVALID
+    assert lib.hp_plan_destroy(None) == hp.HP_OK
+    assert lib.hp_state_step(None, ctypes.c_double(1e-3), 0, 1) == hp.HP_ERR_INVALID
+    assert lib.hp_pendulum_propagate(None, None, None, ctypes.c_double(1e-3), 0, 0) == hp.HP_ERR_INVALID
+
+
+def test_plan_creation_fails_cleanly_without_device(hp):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('a GPU is present')
+    with pytest.raises(hp.HPError) as e:
+        hp.Plan(4, 2, 3)
+    assert e.value.code == hp.HP_ERR_CUDA
+
+
+def test_getu_mirror_matches_oracle(hp):
+    assert np.abs(hp.getu(6) - so3.getu(6)).max() == 0.0
+
+
+def test_mex_argument_checks(hp):
+    P = pd.pendulum_3d(3, 3)
+    hp._check_X(P.X, 3, P.L, 3)
+    with pytest.raises(hp.HPError):
+        hp._check_X(P.X * 1.01, 3, P.L, 3)
+    g = hp._fit_gyro(P.OJO, 3, P.L)
+    J = np.diag(P.params['J'])
+    ref = ((J[1] - J[2]) / J[0], (J[2] - J[0]) / J[1], (J[0] - J[1]) / J[2])
+    assert np.allclose(g, ref, rtol=1e-10, atol=1e-12)
+    Jfull = np.array([[0.02, 0.001, 0.0], [0.001, 0.02, 0.0], [0.0, 0.0, 0.01]])
+    x = pd.omega_grid(3, P.L, 3)
+    with pytest.raises(hp.HPError):
+        hp._fit_gyro(pd.make_OJO(x, Jfull), 3, P.L)
