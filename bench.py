@@ -380,8 +380,16 @@ def main():
         ab = algorithmic_bytes(pmix, fam, True)
         if ab:
             ach = ab / (per / 1e3) / 1e9
+            traffic = None
+            try:
+                with open(os.path.join(ROOT, 'profiles', 'traffic.json')) as fh:
+                    tj = json.load(fh).get(fam)
+                if tj and B == 15 and Bx == 16:
+                    traffic = int(tj['bytes_per_launch'])
+            except Exception:
+                traffic = None
             roof = {'bound': 'hbm', 'kernel': fam, 'achieved': round(ach, 1), 'peak': peaks['hbm_gbs'],
-                    'unit': 'GB/s', 'frac': round(ach / peaks['hbm_gbs'], 4), 'traffic': None,
+                    'unit': 'GB/s', 'frac': round(ach / peaks['hbm_gbs'], 4), 'traffic': traffic,
                     'peak_source': peak_src, 'ms_per_launch': round(per, 4),
                     'algorithmic_bytes_per_launch': int(ab)}
     kernel_ms = {k: round(v[0] / max(v[1], 1), 4) for k, v in prof.items()}

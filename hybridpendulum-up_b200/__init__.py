@@ -38,7 +38,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_fftSO3R_forward', 'hp_fftSO3R_backward', 'hp_pendulum_propagate',
            'hp_pendulum_derivative', 'hp_fftSO3_prod', 'hp_state_create', 'hp_state_destroy',
            'hp_state_load', 'hp_state_store', 'hp_state_step', 'hp_state_density',
-           'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count']
+           'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count',
+           'hp_pendulum_derivative_noalloc', 'hp_state_normalize']
 
 
 class HPError(RuntimeError):
@@ -79,6 +80,7 @@ def _load():
         'hp_plan_profile': [vp, ip],
         'hp_plan_profile_get': [vp, ip, ctypes.c_char_p, ip, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)],
         'hp_plan_launch_count': [vp, ctypes.POINTER(ctypes.c_longlong)],
+        'hp_state_normalize': [vp, dp, ctypes.POINTER(dp)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -296,6 +298,12 @@ class State:
 
     def density_into(self, dev_ptr: int):
         _check(_lib.hp_state_density(self._h, ctypes.c_void_p(dev_ptr)))
+
+    def normalize(self, mass: float) -> float:
+        """Scale the state so its l = 0 mass is `mass`; returns the factor."""
+        f = ctypes.c_double()
+        _check(_lib.hp_state_normalize(self._h, float(mass), ctypes.byref(f)))
+        return f.value
 
     def mass(self) -> float:
         v = ctypes.c_double()

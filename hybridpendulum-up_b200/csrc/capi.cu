@@ -490,6 +490,28 @@ extern "C" int hp_state_density(hp_state* s, void* f) {
   return hp_backward_internal(p, s->F, f, p->symmetry == HP_COMPLEX, p->stream);
 }
 
+__global__ void k_scale_c64(double2* __restrict__ a, long long n, double s) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) { a[i].x *= s; a[i].y *= s; }
+}
+
+extern "C" int hp_state_normalize(hp_state* s, double mass, double* scale) {
+  if (!s || !(mass > 0) || !std::isfinite(mass)) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  double m0 = 0.0;
+  HP_CHECK(hp_state_mass(s, &m0));
+  if (!(m0 > 0) || !std::isfinite(m0)) { hp_set_error("state mass is not positive and finite"); return HP_ERR_NONFINITE; }
+  hp_plan* p = s->plan;
+  const double f = mass / m0;
+  const long long n = p->nrows * p->nx;
+  {
+    ProfScope _ps(p, "normalize", p->stream);
+    k_scale_c64<<<(unsigned)((n + 255) / 256), 256, 0, p->stream>>>(s->F, n, f);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  if (scale) *scale = f;
+  return HP_OK;
+}
+
 extern "C" int hp_state_mass(hp_state* s, double* mass) {
   if (!s || !mass) { hp_set_error("null argument"); return HP_ERR_INVALID; }
   hp_plan* p = s->plan;

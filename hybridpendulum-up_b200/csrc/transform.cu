@@ -127,7 +127,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   const int nrows = (int)L.nrows;
   T* sd = reinterpret_cast<T*>(smraw);
   C* sG = reinterpret_cast<C*>(smraw + ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16);
-  const int b0 = blockIdx.y * NB;
+  // beta groups of one omega chunk are consecutive blocks, so they read the
+  // same coefficient rows close together in time (L2 reuse)
+  constexpr int NGROUPS = (NB2 + NB - 1) / NB;
+  const int grp = blockIdx.x % NGROUPS;
+  const int chunk = blockIdx.x / NGROUPS;
+  const int b0 = grp * NB;
   const int nbv = min(NB, NB2 - b0);
   const int tid = threadIdx.x, nth = blockDim.x;
   for (int e = tid; e < NB * nrows; e += nth) {   // interleaved [row][bb]
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   }
   const long long nx = L.nx;
   for (int bt = 0; bt < nbatch; ++bt) {
-    const long long w0 = ((long long)blockIdx.x * nbatch + bt) * P;
+    const long long w0 = ((long long)chunk * nbatch + bt) * P;
     if (w0 >= nx) break;
     __syncthreads();
     // beta stage: item (pair, p), p fastest
@@ -469,7 +474,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
   gx = (nbatches + nbatch - 1) / nbatch;
   HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)gx, (unsigned)ngroups);
+  dim3 grid((unsigned)(gx * ngroups), 1);
   ProfScope _ps(p, "tf.synth", s);
   k_synth<B, T, NB, P, CPLX><<<grid, 256, smem, s>>>(p->layout(), Fp,
                                                      p->precision == HP_FP64 ? (const T*)(const void*)p->wig64

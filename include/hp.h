@@ -171,6 +171,12 @@ int hp_state_step(hp_state* state, double dt, int method, int nsteps);
 int hp_state_density(hp_state* state, void* f);
 /* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
 int hp_state_mass(hp_state* state, double* mass);
+/* l = 0 mass normalisation: scales the state (FP64) so that F^0_{00}[0] == mass;
+ * *scale (may be NULL) receives the factor applied.  The derivative conserves
+ * F^0_{00}[0] exactly (every term vanishes at l = 0, k = 0), so this only
+ * corrects changes made outside the propagation (grid-side collision updates,
+ * truncation of a user-supplied density).  No counterpart in the reference. */
+int hp_state_normalize(hp_state* state, double mass, double* scale);
 
 #ifdef __cplusplus
 }

@@ -169,6 +169,19 @@ def test_state_multistep_and_mass(hp):
     assert abs(st.mass() - m0) < 1e-12 * abs(m0)
 
 
+def test_state_normalize(hp):
+    P = pd.pendulum_3d(3, 2)
+    f, _ = pd.seeded_density(3, 2, 3, P.L, seed=12)
+    F = so3.fftSO3R_forward(f)
+    st = hp.State(_model3(hp, P, 0))
+    st.load(F)
+    m0 = st.mass()
+    fac = st.normalize(2.0 * m0)
+    assert abs(fac - 2.0) < 1e-14
+    assert abs(st.mass() - 2.0 * m0) < 1e-13 * abs(m0)
+    assert rel(st.store(), 2.0 * F) < 1e-14
+
+
 @pytest.mark.parametrize('B', [2, 4, 6])
 def test_fftSO3_prod(hp, B):
     F = random_coeffs(B, (), seed=B)
