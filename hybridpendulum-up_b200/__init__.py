@@ -39,7 +39,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_derivative', 'hp_fftSO3_prod', 'hp_state_create', 'hp_state_destroy',
            'hp_state_load', 'hp_state_store', 'hp_state_step', 'hp_state_density',
            'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count',
-           'hp_pendulum_derivative_noalloc', 'hp_state_normalize']
+           'hp_pendulum_derivative_noalloc', 'hp_state_normalize', 'hp_collision_create',
+           'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df']
 
 
 class HPError(RuntimeError):
@@ -51,6 +52,12 @@ class HPError(RuntimeError):
 class hp_model(ctypes.Structure):
     _fields_ = [('L', ctypes.c_double), ('b', ctypes.c_double * 3), ('G', ctypes.c_double * 9),
                 ('gyro', ctypes.c_double * 3)]
+
+
+class hp_collision_params(ctypes.Structure):
+    _fields_ = [('d', ctypes.c_double), ('h', ctypes.c_double), ('r', ctypes.c_double),
+                ('theta_t', ctypes.c_double), ('lambda_max', ctypes.c_double), ('epsilon', ctypes.c_double),
+                ('L', ctypes.c_double), ('Gd', ctypes.c_double * 4), ('nD', ctypes.c_int)]
 
 
 class hp_plan_info_t(ctypes.Structure):
@@ -81,6 +88,10 @@ def _load():
         'hp_plan_profile_get': [vp, ip, ctypes.c_char_p, ip, ctypes.POINTER(dp), ctypes.POINTER(ctypes.c_longlong)],
         'hp_plan_launch_count': [vp, ctypes.POINTER(ctypes.c_longlong)],
         'hp_state_normalize': [vp, dp, ctypes.POINTER(dp)],
+        'hp_collision_create': [vp, ctypes.POINTER(hp_collision_params), ctypes.POINTER(vp), ctypes.POINTER(ip)],
+        'hp_collision_destroy': [vp],
+        'hp_collision_tables': [vp, vp, vp, vp, vp, vp, vp, ip],
+        'hp_collision_df': [vp, vp, vp, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -326,6 +337,49 @@ def _empty_like_mem(ref, shape, dtype):
     import torch
     tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.complex128): torch.complex128}[np.dtype(dtype)]
     return torch.zeros(int(np.prod(shape)), dtype=tdt, device=ref.device)
+
+
+class Collision:
+    """Hybrid collision operator of pendulum_reduced_hybrid on a 2-D plan:
+    getLambda_mex + getOmega_mex('new') + getFcL_mex tables, and the per-step
+    pendulum_reduced_discrete_propagate(true, f, ...)."""
+
+    def __init__(self, plan: Plan, d, h, r, theta_t, lambda_max, epsilon, L, Gd, nD=10):
+        p = hp_collision_params()
+        p.d, p.h, p.r, p.theta_t, p.lambda_max, p.epsilon, p.L = d, h, r, theta_t, lambda_max, epsilon, L
+        g = np.asarray(Gd, float).reshape(2, 2).ravel(order='F')
+        for i in range(4):
+            p.Gd[i] = g[i]
+        p.nD = int(nD)
+        hnd, n = ctypes.c_void_p(), ctypes.c_int()
+        _check(_lib.hp_collision_create(plan.handle, ctypes.byref(p), ctypes.byref(hnd), ctypes.byref(n)))
+        self._h, self.plan, self.numR, self.nD = hnd, plan, n.value, int(nD)
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h is not None and _lib is not None:
+            _lib.hp_collision_destroy(h)
+            self._h = None
+
+    def tables(self):
+        nx = self.plan.N ** 2
+        k, nD = self.numR, self.nD
+        lam = np.zeros((nx, k)); ind = np.zeros(k, np.int32); om = np.zeros((nx, k, 2))
+        fcL = np.zeros((nx, k, nD)); idx = np.zeros((nx, k, nD), np.int16)
+        PC = np.zeros((8 * self.plan.B ** 3, 3))
+        ptrs = [ctypes.c_void_p(a.ctypes.data) for a in (lam, ind, om, fcL, idx, PC)]
+        _check(_lib.hp_collision_tables(self._h, *ptrs, HP_HOST))
+        return dict(lambda_=lam, indR=ind, omega=om, fcL=fcL, fcL_indx=idx, PC=PC)
+
+    def df(self, f, out=None):
+        """f: density f(a,b,c,i,j) (MATLAB layout); returns df, same layout."""
+        f = _as_matlab(f, np.float64)
+        if out is None:
+            out = _empty_like_mem(f, self.plan.f_shape, np.float64)
+        pf, mf = _ptr(f, np.float64)
+        po, _ = _ptr(out, np.float64)
+        _check(_lib.hp_collision_df(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(po), mf))
+        return out
 
 
 @lru_cache(maxsize=32)

@@ -1,0 +1,306 @@
+// Hybrid collision operator of pendulum_reduced_hybrid (2-D reduced Omega):
+// switching rate lambda(R, x), reset map Omega+, truncated Gaussian kernel fcL
+// and the per-step update df = sum_d fcL f(R, idx) - lambda f (FP64, as the
+// reference).  Follows propagation/discrete/mex/sources/pendulum_reduced_collision:
+// getLambda.cu:8-85,192-267, getOmega.cu:64-103, getFcL.cu:11-166,
+// propagate.cu:6-121,181-231.
+//
+// Layouts (those of the reference MEX):
+//   f, df         [ix][iR]      ix = i + 2Bx j, iR = a + 2B b + 4B^2 c
+//   lambda        [ix][k]       k indexes the colliding attitudes indR
+//   fcL, fcL_idx  [ix][k][d]    d < nD
+#include <cmath>
+#include <vector>
+#include "common.cuh"
+#include "plan.hpp"
+
+using namespace hp;
+
+struct CollisionTables {
+  int numR = 0, nD = 0;
+  int* indR = nullptr;        // [numR]
+  double* lambda = nullptr;   // [nx][numR]
+  double* omega = nullptr;    // [nx][numR][2]
+  double* fcL = nullptr;      // [nx][numR][nD]
+  short* idx = nullptr;       // [nx][numR][nD]
+  double* PC = nullptr;       // [nR][3]
+};
+
+static CollisionTables g_dummy;
+
+// R(:,:,a,b,c) = Rz(alpha_a) Ry(beta_b) Rz(gamma_c) as in fftSO3R.m:30-47.
+__device__ __forceinline__ void rot_of(int iR, int B, double R[3][3]) {
+  const int n = 2 * B;
+  const int a = iR % n, b = (iR / n) % n, c = iR / (n * n);
+  const double al = M_PI / B * a, be = M_PI / (4.0 * B) * (2 * b + 1), ga = M_PI / B * c;
+  const double ca = cos(al), sa = sin(al), cb = cos(be), sb = sin(be), cg = cos(ga), sg = sin(ga);
+  const double Ra[3][3] = {{ca, -sa, 0}, {sa, ca, 0}, {0, 0, 1}};
+  const double Rb[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+  const double Rg[3][3] = {{cg, -sg, 0}, {sg, cg, 0}, {0, 0, 1}};
+  double T[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) T[i][j] = Ra[i][0] * Rb[0][j] + Ra[i][1] * Rb[1][j] + Ra[i][2] * Rb[2][j];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) R[i][j] = T[i][0] * Rg[0][j] + T[i][1] * Rg[1][j] + T[i][2] * Rg[2][j];
+}
+
+// Category (0: none, 1: ramp, 2: full), theta = asin(R13) and PC per attitude.
+__global__ void k_coll_theta(int B, int nR, double theta0, double thetat, double h, double r, char* cat,
+                             double* theta, double* PC) {
+  const int iR = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iR >= nR) return;
+  double R[3][3];
+  rot_of(iR, B, R);
+  const double th = asin(R[0][2]);
+  theta[iR] = th;
+  cat[iR] = th < theta0 - thetat ? 0 : (th > theta0 + thetat ? 2 : 1);
+  const double lr3 = h - r * tan(th);
+  PC[3 * iR] = lr3 * R[0][2] + r / cos(th);
+  PC[3 * iR + 1] = lr3 * R[1][2];
+  PC[3 * iR + 2] = lr3 * R[2][2];
+}
+
+// lambda(ix, k) and Omega+(ix, k) for the colliding attitudes.
+__global__ void k_coll_lambda_omega(int B, int N, double L, int numR, const int* __restrict__ indR,
+                                    const char* __restrict__ cat, const double* __restrict__ theta,
+                                    const double* __restrict__ PC, double theta0, double thetat, double lmax,
+                                    double eps, double* __restrict__ lambda, double* __restrict__ omega) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nx = N * N;
+  if (t >= (long long)nx * numR) return;
+  const int k = (int)(t % numR), ix = (int)(t / numR);
+  const int iR = indR[k];
+  double R[3][3];
+  rot_of(iR, B, R);
+  const double x1 = -L / 2 + L / N * (ix % N), x2 = -L / 2 + L / N * (ix / N);
+  double lam = cat[iR] == 2 ? lmax : lmax / 2 * sin(M_PI / (2 * thetat) * (theta[iR] - theta0)) + lmax / 2;
+  if (cat[iR] == 0) lam = 0.0;
+  const double o0 = R[1][0] * x1 + R[1][1] * x2, o1 = R[2][0] * x1 + R[2][1] * x2;
+  const double vC = o0 * PC[3 * iR + 2] - o1 * PC[3 * iR + 1];
+  lambda[t] = vC < 0.0 ? 0.0 : lam;
+  // reset map
+  const double nt = sqrt(R[1][2] * R[1][2] + R[2][2] * R[2][2]);
+  const double t1 = R[2][2] / nt, t2 = -R[1][2] / nt;
+  const double w0 = R[0][0] * x1 + R[0][1] * x2;
+  double w1 = R[1][0] * x1 + R[1][1] * x2, w2 = R[2][0] * x1 + R[2][1] * x2;
+  const double ot = (1.0 + eps) * (w1 * t1 + w2 * t2);
+  w1 -= ot * t1;
+  w2 -= ot * t2;
+  omega[2 * t] = R[0][0] * w0 + R[1][0] * w1 + R[2][0] * w2;
+  omega[2 * t + 1] = R[0][1] * w0 + R[1][1] * w1 + R[2][1] * w2;
+}
+
+// Largest nD Gaussian taps per (landing point ix1, attitude k), ties keeping the
+// lower source index first (the stable descending sort of getFcL.cu:76).
+template <int MAXD>
+__global__ void k_coll_topd(int N, double L, int numR, int nD, const double* __restrict__ omega, double i00,
+                            double i01, double i11, double cn, double* __restrict__ fcL, short* __restrict__ idx) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int nx = N * N;
+  if (t >= (long long)nx * numR) return;
+  const int k = (int)(t % numR), ix1 = (int)(t / numR);
+  const double x1 = -L / 2 + L / N * (ix1 % N), x2 = -L / 2 + L / N * (ix1 / N);
+  double v[MAXD];
+  int id[MAXD];
+  int cnt = 0;
+  for (int ix2 = 0; ix2 < nx; ++ix2) {
+    const double d0 = x1 - omega[2 * ((long long)ix2 * numR + k)];
+    const double d1 = x2 - omega[2 * ((long long)ix2 * numR + k) + 1];
+    const double q = i00 * d0 * d0 + i01 * d0 * d1 + i11 * d1 * d1;
+    const double fc = exp(-0.5 * q) * cn;
+    if (cnt < nD || fc > v[nD - 1]) {
+      int p = cnt < nD ? cnt++ : nD - 1;      // insertion position from the end
+      while (p > 0 && v[p - 1] < fc) {         // strict: equal values keep the earlier index first
+        v[p] = v[p - 1];
+        id[p] = id[p - 1];
+        --p;
+      }
+      v[p] = fc;
+      id[p] = ix2;
+    }
+  }
+  for (int d = 0; d < nD; ++d) {
+    fcL[t * nD + d] = d < cnt ? v[d] : 0.0;
+    idx[t * nD + d] = (short)(d < cnt ? id[d] : 0);
+  }
+}
+
+__global__ void k_coll_norm(int nx, int numR, int nD, const double* __restrict__ fcL, const short* __restrict__ idx,
+                            double* __restrict__ norm) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * numR * nD) return;
+  const int k = (int)((t / nD) % numR);
+  atomicAdd(&norm[(long long)idx[t] * numR + k], fcL[t]);
+}
+
+__global__ void k_coll_scale(int nx, int numR, int nD, double dx2, const double* __restrict__ norm,
+                             const double* __restrict__ lambda, double* __restrict__ fcL, const short* __restrict__ idx) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * numR * nD) return;
+  const int k = (int)((t / nD) % numR);
+  const long long src = (long long)idx[t] * numR + k;
+  fcL[t] = fcL[t] / (norm[src] * dx2) * (lambda[src] * dx2);
+}
+
+// df(R_k, x) = sum_d fcL f(R_k, idx) - lambda f(R_k, x); rows of non-colliding
+// attitudes are left as the caller set them (zero).
+template <typename T>
+__global__ void k_coll_df(int nx, int nR, int numR, int nD, const int* __restrict__ indR,
+                          const double* __restrict__ lambda, const double* __restrict__ fcL,
+                          const short* __restrict__ idx, const T* __restrict__ f, T* __restrict__ df) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * numR) return;
+  const int k = (int)(t % numR), ix = (int)(t / numR);
+  const int iR = indR[k];
+  double s = 0.0;
+  for (int d = 0; d < nD; ++d) s += fcL[t * nD + d] * (double)f[(long long)idx[t * nD + d] * nR + iR];
+  df[(long long)ix * nR + iR] = (T)(s - lambda[t] * (double)f[(long long)ix * nR + iR]);
+}
+
+// --------------------------------------------------------------- C ABI ----
+struct hp_collision {
+  hp_plan* plan = nullptr;
+  CollisionTables t;
+  double L = 0;
+};
+
+extern "C" int hp_collision_create(hp_plan* p, const hp_collision_params* prm, hp_collision** out, int* numR) {
+  if (!p || !prm || !out) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  *out = nullptr;
+  if (p->ndim != 2) { hp_set_error("the collision operator is defined for the 2-D reduced model"); return HP_ERR_UNSUPPORTED; }
+  if (prm->nD < 1 || prm->nD > 32) { hp_set_error("nD must be in 1..32"); return HP_ERR_INVALID; }
+  if (!(prm->L > 0) || !(prm->theta_t > 0)) { hp_set_error("bad collision parameters"); return HP_ERR_INVALID; }
+  const int B = p->B, N = p->N, nR = 8 * B * B * B, nx = N * N;
+  cudaStream_t s = p->stream;
+  const double hr = std::sqrt(prm->h * prm->h + prm->r * prm->r);
+  const double theta0 = std::asin(prm->d / hr) - std::asin(prm->r / hr);
+  char* cat = nullptr;
+  double* theta = nullptr;
+  hp_collision* c = new hp_collision();
+  c->plan = p;
+  c->L = prm->L;
+  auto fail = [&](int code) { hp_collision_destroy(c); cudaFree(cat); cudaFree(theta); return code; };
+  if (cudaMalloc(&cat, nR) != cudaSuccess || cudaMalloc(&theta, sizeof(double) * nR) != cudaSuccess ||
+      cudaMalloc(&c->t.PC, sizeof(double) * 3 * nR) != cudaSuccess) {
+    cudaGetLastError();
+    hp_set_error("device allocation failed");
+    return fail(HP_ERR_ALLOC);
+  }
+  {
+    ProfScope _ps(p, "coll.setup", s);
+    k_coll_theta<<<(nR + 127) / 128, 128, 0, s>>>(B, nR, theta0, prm->theta_t, prm->h, prm->r, cat, theta, c->t.PC);
+  }
+  std::vector<char> hc(nR);
+  if (cudaMemcpyAsync(hc.data(), cat, nR, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    hp_set_error(cudaGetErrorString(cudaGetLastError()));
+    return fail(HP_ERR_CUDA);
+  }
+  std::vector<int> hind;
+  for (int i = 0; i < nR; ++i) if (hc[i] != 0) hind.push_back(i);
+  const int nk = (int)hind.size();
+  c->t.numR = nk;
+  c->t.nD = prm->nD;
+  if (numR) *numR = nk;
+  if (nk == 0) { cudaFree(cat); cudaFree(theta); *out = c; return HP_OK; }
+  const size_t nxk = (size_t)nx * nk;
+  double* norm = nullptr;
+  if (cudaMalloc(&c->t.indR, sizeof(int) * nk) != cudaSuccess ||
+      cudaMalloc(&c->t.lambda, sizeof(double) * nxk) != cudaSuccess ||
+      cudaMalloc(&c->t.omega, sizeof(double) * 2 * nxk) != cudaSuccess ||
+      cudaMalloc(&c->t.fcL, sizeof(double) * nxk * prm->nD) != cudaSuccess ||
+      cudaMalloc(&c->t.idx, sizeof(short) * nxk * prm->nD) != cudaSuccess ||
+      cudaMalloc(&norm, sizeof(double) * nxk) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(norm);
+    hp_set_error("device allocation failed");
+    return fail(HP_ERR_ALLOC);
+  }
+  HP_CUDA_TRY(cudaMemcpyAsync(c->t.indR, hind.data(), sizeof(int) * nk, cudaMemcpyHostToDevice, s));
+  const unsigned g1 = (unsigned)((nxk + 127) / 128);
+  {
+    ProfScope _ps(p, "coll.setup", s);
+    k_coll_lambda_omega<<<g1, 128, 0, s>>>(B, N, prm->L, nk, c->t.indR, cat, theta, c->t.PC, theta0, prm->theta_t,
+                                           prm->lambda_max, prm->epsilon, c->t.lambda, c->t.omega);
+  }
+  // Gaussian of covariance Gd (column-major 2x2)
+  const double g00 = prm->Gd[0], g10 = prm->Gd[1], g01 = prm->Gd[2], g11 = prm->Gd[3];
+  const double det = g00 * g11 - g01 * g10;
+  if (!(det > 0)) { cudaFree(norm); hp_set_error("Gd must be positive definite"); return fail(HP_ERR_INVALID); }
+  const double cn = 1.0 / (2 * M_PI * std::sqrt(det));
+  const double i00 = g11 / det, i01 = (-g01 - g10) / det, i11 = g00 / det;
+  {
+    ProfScope _ps(p, "coll.setup", s);
+    k_coll_topd<32><<<g1, 128, 0, s>>>(N, prm->L, nk, prm->nD, c->t.omega, i00, i01, i11, cn, c->t.fcL, c->t.idx);
+  }
+  const double dx = prm->L / N, dx2 = dx * dx;
+  HP_CUDA_TRY(cudaMemsetAsync(norm, 0, sizeof(double) * nxk, s));
+  const unsigned g2 = (unsigned)((nxk * prm->nD + 127) / 128);
+  {
+    ProfScope _ps(p, "coll.setup", s);
+    k_coll_norm<<<g2, 128, 0, s>>>(nx, nk, prm->nD, c->t.fcL, c->t.idx, norm);
+    k_coll_scale<<<g2, 128, 0, s>>>(nx, nk, prm->nD, dx2, norm, c->t.lambda, c->t.fcL, c->t.idx);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(norm);
+  cudaFree(cat);
+  cudaFree(theta);
+  *out = c;
+  return HP_OK;
+}
+
+extern "C" int hp_collision_destroy(hp_collision* c) {
+  if (!c) return HP_OK;
+  cudaFree(c->t.indR); cudaFree(c->t.lambda); cudaFree(c->t.omega); cudaFree(c->t.fcL);
+  cudaFree(c->t.idx); cudaFree(c->t.PC);
+  delete c;
+  return HP_OK;
+}
+
+extern "C" int hp_collision_tables(hp_collision* c, double* lambda, int* indR, double* omega, double* fcL,
+                                   short* fcL_indx, double* PC, int mem) {
+  if (!c) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("bad mem"); return HP_ERR_INVALID; }
+  hp_plan* p = c->plan;
+  const cudaMemcpyKind kind = mem == HP_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t nxk = (size_t)p->N * p->N * c->t.numR;
+  const int nR = 8 * p->B * p->B * p->B;
+  if (lambda && nxk) HP_CUDA_TRY(cudaMemcpy(lambda, c->t.lambda, sizeof(double) * nxk, kind));
+  if (indR && c->t.numR) HP_CUDA_TRY(cudaMemcpy(indR, c->t.indR, sizeof(int) * c->t.numR, kind));
+  if (omega && nxk) HP_CUDA_TRY(cudaMemcpy(omega, c->t.omega, sizeof(double) * 2 * nxk, kind));
+  if (fcL && nxk) HP_CUDA_TRY(cudaMemcpy(fcL, c->t.fcL, sizeof(double) * nxk * c->t.nD, kind));
+  if (fcL_indx && nxk) HP_CUDA_TRY(cudaMemcpy(fcL_indx, c->t.idx, sizeof(short) * nxk * c->t.nD, kind));
+  if (PC) HP_CUDA_TRY(cudaMemcpy(PC, c->t.PC, sizeof(double) * 3 * nR, kind));
+  return HP_OK;
+}
+
+extern "C" int hp_collision_df(hp_collision* c, const double* f, double* df, int mem) {
+  if (!c || !f || !df) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("bad mem"); return HP_ERR_INVALID; }
+  hp_plan* p = c->plan;
+  const long long nR = 8LL * p->B * p->B * p->B, nx = (long long)p->N * p->N, n = nR * nx;
+  int st = HP_OK;
+  const double* fd = f;
+  double* dd = df;
+  if (mem == HP_HOST) {
+    double* a = (double*)p->ws_get("coll.f", sizeof(double) * n, &st);
+    if (st) return st;
+    double* b = (double*)p->ws_get("coll.df", sizeof(double) * n, &st);
+    if (st) return st;
+    HP_CUDA_TRY(cudaMemcpyAsync(a, f, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
+    fd = a;
+    dd = b;
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(dd, 0, sizeof(double) * n, p->stream));
+  if (c->t.numR > 0) {
+    const long long nt = nx * c->t.numR;
+    ProfScope _ps(p, "coll.df", p->stream);
+    k_coll_df<double><<<(unsigned)((nt + 255) / 256), 256, 0, p->stream>>>(
+        (int)nx, (int)nR, c->t.numR, c->t.nD, c->t.indR, c->t.lambda, c->t.fcL, c->t.idx, fd, dd);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  if (mem == HP_HOST) HP_CUDA_TRY(cudaMemcpyAsync(df, dd, sizeof(double) * n, cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}

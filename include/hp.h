@@ -157,6 +157,36 @@ int hp_pendulum_derivative_noalloc(hp_plan* plan, const double* F, double* dF);
 int hp_fftSO3_prod(hp_plan* plan, const double* F, const double* G, double* FG, int batch,
                    int mem);
 
+/* ---- hybrid collision operator (2-D reduced model, FP64) ----
+ * hp_collision_create builds the one-time tables of the reference's
+ *   [lambda,indR,PC] = getLambda_mex(R,x,dWall,h,r,theta_t,lambda_max,false)
+ *     (propagation/discrete/mex/sources/pendulum_reduced_collision/src/getLambda.cu:8-85)
+ *   Omega_new = getOmega_mex(R,x,indR,epsilon,PC,'new')      (.../src/getOmega.cu:8-103)
+ *   [fcL,fcL_indx] = getFcL_mex(x,Omega_new,lambda,Gd,nD)    (.../src/getFcL.cu:11-166)
+ * on the plan's SO(3) grid and its omega grid of period L (callers:
+ * propagation/pendulum_reduced_hybrid.m:130-142).  *numR receives the number
+ * of colliding attitudes.  hp_collision_df is
+ *   df = pendulum_reduced_discrete_propagate(true,f,lambda,indR,fcL,fcL_indx)
+ *     (.../src/mexPropagate.cpp:6-77, propagate.cu:6-121; caller pendulum_reduced_hybrid.m:232)
+ * with f, df real grid densities f(a,b,c,i,j).  hp_collision_tables copies the
+ * tables out in the MEX layouts: lambda [ix][k], indR [k] (0-based), omega
+ * [ix][k][2], fcL and fcL_indx [ix][k][d], PC [iR][3]; NULL skips a table. */
+typedef struct hp_collision hp_collision;
+typedef struct {
+  double d, h, r;          /* wall distance, pivot-to-tip height, tip radius */
+  double theta_t;          /* half width of the switching ramp (rad)       */
+  double lambda_max;       /* maximum switching rate                       */
+  double epsilon;          /* coefficient of restitution                   */
+  double L;                /* omega-grid period                            */
+  double Gd[4];            /* reset-noise covariance, column-major 2x2     */
+  int nD;                  /* taps kept per landing point (<= 32)          */
+} hp_collision_params;
+int hp_collision_create(hp_plan* plan, const hp_collision_params* params, hp_collision** coll, int* numR);
+int hp_collision_destroy(hp_collision* coll);
+int hp_collision_tables(hp_collision* coll, double* lambda, int* indR, double* omega, double* fcL,
+                        short* fcL_indx, double* PC, int mem);
+int hp_collision_df(hp_collision* coll, const double* f, double* df, int mem);
+
 /* ---- resident state: coefficients kept on the device in the plan's internal
  * layout across steps (the time loops of pendulum.m:269-315 and
  * pendulum_reduced.m:243-289 without host round trips). ---- */
