@@ -40,7 +40,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_state_load', 'hp_state_store', 'hp_state_step', 'hp_state_density',
            'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count',
            'hp_pendulum_derivative_noalloc', 'hp_state_normalize', 'hp_collision_create',
-           'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df']
+           'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
+           'hp_pendulum_propagate_den', 'hp_state_hybrid_step']
 
 
 class HPError(RuntimeError):
@@ -92,6 +93,9 @@ def _load():
         'hp_collision_destroy': [vp],
         'hp_collision_tables': [vp, vp, vp, vp, vp, vp, vp, ip],
         'hp_collision_df': [vp, vp, vp, ip],
+        'hp_plan_set_den_model': [vp, ctypes.POINTER(hp_model), vp, ip],
+        'hp_pendulum_propagate_den': [vp, vp, vp, vp, dp, ip, ip],
+        'hp_state_hybrid_step': [vp, vp, dp, ip, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -187,6 +191,28 @@ class Plan:
         self.model = dict(L=float(L), b=np.array(bb[:3]), G=Gm, gyro=tuple(gyro))
         self._MR_keep = MRc
 
+    def set_den_model(self, L: float, b, G, mR):
+        """Density-gravity model of pendulum_reduced_den.m (2-D plans): the
+        gravity term fftSO3R(f . mR_i) is formed on the grid.  mR: (2, 2B, 2B, 2B)
+        real samples (pendulum_reduced_den.m:132)."""
+        m = hp_model()
+        m.L = float(L)
+        bb = list(np.asarray(b, float).ravel()) + [0.0] * 3
+        for i in range(3):
+            m.b[i] = bb[i]
+        Gm = np.zeros((3, 3))
+        Ga = np.asarray(G, float)
+        Gm[:Ga.shape[0], :Ga.shape[1]] = Ga
+        for i in range(9):
+            m.G[i] = Gm.ravel()[i]
+        mRc = _as_matlab(mR, np.float64)
+        if tuple(mRc.shape) != (2,) + (2 * self.B,) * 3:
+            raise HPError(HP_ERR_SHAPE, f'mR must have shape (2, {2 * self.B}, {2 * self.B}, {2 * self.B})')
+        p, mem = _ptr(mRc, np.float64)
+        _check(_lib.hp_plan_set_den_model(self._h, ctypes.byref(m), ctypes.c_void_p(p), mem))
+        self.model = dict(L=float(L), b=np.array(bb[:3]), G=Gm, gyro=(0.0, 0.0, 0.0))
+        self._MR_keep = mRc
+
     def profile(self, enable: bool = True):
         """Start (and reset) or stop per-kernel-family CUDA-event timing."""
         _check(_lib.hp_plan_profile(self._h, int(enable)))
@@ -255,6 +281,26 @@ class Plan:
                                           METHODS[method.lower()], mi))
         return out
 
+    def propagate_den(self, F, f, dt: float, method: str = 'euler', out=None):
+        """One step of the density-gravity model; f is the grid density of F
+        (None: recomputed from F by the backward transform)."""
+        F = _as_matlab(F, np.complex128)
+        if out is None:
+            out = _empty_like_mem(F, self.F_shape, np.complex128)
+        pi, mi = _ptr(F, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        pf = None
+        if f is not None:
+            f = _as_matlab(f, np.float64)
+            if tuple(f.shape) != tuple(self.f_shape):
+                raise HPError(HP_ERR_SHAPE, f'f must have shape {self.f_shape}')
+            pf, mf = _ptr(f, np.float64)
+            if mf != mi:
+                raise ValueError('F and f must live in the same memory space')
+        _check(_lib.hp_pendulum_propagate_den(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(pf),
+                                              ctypes.c_void_p(po), float(dt), METHODS[method.lower()], mi))
+        return out
+
     def derivative(self, F, out=None):
         F = _as_matlab(F, np.complex128)
         if out is None:
@@ -306,6 +352,13 @@ class State:
 
     def step(self, dt: float, method: str = 'euler', nsteps: int = 1):
         _check(_lib.hp_state_step(self._h, float(dt), METHODS[method.lower()], int(nsteps)))
+
+    def hybrid_step(self, coll: 'Collision', dt: float, method: str = 'euler', nsteps: int = 1):
+        """nsteps steps of pendulum_reduced_hybrid.m:224-234 (density-gravity
+        propagation, backward transform, collision update, forward transform)."""
+        if coll.plan is not self.plan:
+            raise ValueError('the collision operator must be built on the state plan')
+        _check(_lib.hp_state_hybrid_step(self._h, coll._h, float(dt), METHODS[method.lower()], int(nsteps)))
 
     def density_into(self, dev_ptr: int):
         _check(_lib.hp_state_density(self._h, ctypes.c_void_p(dev_ptr)))
@@ -479,6 +532,31 @@ def pendulum_propagate_reduced(F, X, MR, bt, G, dt, L, u, CG, method='euler'):
 def pendulum_propagate_reduced32(F, X, MR, bt, G, dt, L, u, CG, method='euler'):
     plan = _model_plan(F, X, None, MR, bt, G, L, HP_MIXED)
     return plan.propagate(F, dt, method)
+
+
+def _den_plan(F, X, mR, b, G, L, precision):
+    F = np.asarray(F)
+    B, Bx, ndim = F.shape[2], F.shape[3] // 2, F.ndim - 3
+    if ndim != 2:
+        raise HPError(HP_ERR_SHAPE, 'the density-gravity model is the reduced (2-D) pendulum')
+    _check_X(X, Bx, L, ndim)
+    plan = get_plan(B, Bx, ndim, precision, HP_REAL)
+    plan.set_den_model(L, b, G, mR)
+    return plan
+
+
+def pendulum_propagate_reduced_den(F, f, X, mR, bt, G, dt, L, u, d, w, method='euler'):
+    """Drop-in for pendulum_propagate_reduced_den(F,f,X,mR,bt,G,dt,L,u,d,w,method)
+    (propagation/mex/sources/pendulum_propagate_reduced_den/kernel.cu:9-325).
+    u, d and w are accepted for signature compatibility; f may be None."""
+    plan = _den_plan(F, X, mR, bt, G, L, HP_FP64)
+    return plan.propagate_den(F, f, dt, method)
+
+
+def pendulum_propagate_reduced_den32(F, f, X, mR, bt, G, dt, L, u, d, w, method='euler'):
+    """Mixed-precision twin of pendulum_propagate_reduced_den."""
+    plan = _den_plan(F, X, mR, bt, G, L, HP_MIXED)
+    return plan.propagate_den(F, f, dt, method)
 
 
 def fftSO3R_mex(direction: str, A, d=None, w=None, precision: int = HP_FP64):

@@ -238,6 +238,41 @@ extern "C" int hp_plan_set_model(hp_plan* p, const hp_model* m, const double* MR
   HP_CHECK(hp_build_gravity_taps(p, dMR));
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   p->model = *m;
+  p->den_mR = nullptr;
+  p->has_model = true;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_set_den_model(hp_plan* p, const hp_model* m, const double* mR, int mem) {
+  if (!p || !m || !mR) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  if (p->ndim != 2 || p->symmetry != HP_REAL) {
+    hp_set_error("density gravity needs a 2-D plan with HP_REAL symmetry");
+    return HP_ERR_UNSUPPORTED;
+  }
+  if (!(m->L > 0) || !std::isfinite(m->L)) { hp_set_error("L must be positive"); return HP_ERR_INVALID; }
+  const size_t ng = (size_t)8 * p->B * p->B * p->B;
+  std::vector<double> h(2 * ng), dein(2 * ng);
+  if (mem == HP_HOST) std::memcpy(h.data(), mR, sizeof(double) * 2 * ng);
+  else HP_CUDA_TRY(cudaMemcpy(h.data(), mR, sizeof(double) * 2 * ng, cudaMemcpyDeviceToHost));
+  for (size_t e = 0; e < ng; ++e)
+    for (int i = 0; i < 2; ++i) {
+      const double v = h[2 * e + i];  // mR(i, a, b, c), component fastest
+      if (!std::isfinite(v)) { hp_set_error("mR has non-finite entries"); return HP_ERR_NONFINITE; }
+      dein[i * ng + e] = v;
+    }
+  int st = HP_OK;
+  double* d = (double*)p->ws_get("model.denmR", sizeof(double) * 2 * ng, &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaMemcpy(d, dein.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice));
+  const size_t nMR = (size_t)p->D * p->D * (p->lmax + 1) * p->ndim;
+  double2* dMR = (double2*)p->ws_get("model.MR", sizeof(double2) * nMR, &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaMemsetAsync(dMR, 0, sizeof(double2) * nMR, p->stream));
+  HP_CHECK(hp_build_gravity_taps(p, dMR));  // no coefficient-space gravity
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  p->model = *m;
+  p->den_mR = d;
   p->has_model = true;
   return HP_OK;
 }
@@ -327,29 +362,32 @@ extern "C" int hp_fftSO3R_backward(hp_plan* p, const double* F, double* f, int m
 // ----------------------------------------------------------- integrators ----
 // One step of `method` on internal-layout buffers; the result lands in *F
 // (buffers are swapped, never aliased inside one derivative evaluation).
+// fgrid: grid density of *F for the first stage of a density-gravity model
+// (null: recomputed from *F), as pendulum_reduced_den.m:359-399 passes f to the
+// first derivative only.
 static int integrate_internal(hp_plan* p, double2** F, double2** F2, double2** F3, double2* acc, double dt,
-                              int method) {
+                              int method, const void* fgrid = nullptr) {
   cudaStream_t s = p->stream;
   const size_t bytes = 16 * (size_t)p->nrows * p->nx;
   switch (method) {
     case HP_EULER:
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, nullptr, 0.0, s, fgrid));
       std::swap(*F, *F2);
       return HP_OK;
     case HP_MIDPOINT:
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, nullptr, 0.0, s, fgrid));
       HP_CHECK(hp_derivative_eval(p, *F2, *F, dt, *F3, nullptr, 0.0, s));
       std::swap(*F, *F3);
       return HP_OK;
     case HP_RK2:
       HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, acc, dt / 2, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, acc, dt / 2, s, fgrid));
       HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 2, *F3, nullptr, 0.0, s));
       std::swap(*F, *F3);
       return HP_OK;
     case HP_RK4:
       HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, acc, dt / 6, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, acc, dt / 6, s, fgrid));
       HP_CHECK(hp_derivative_eval(p, *F2, *F, dt / 2, *F3, acc, dt / 3, s));
       HP_CHECK(hp_derivative_eval(p, *F3, *F, dt, *F2, acc, dt / 3, s));
       HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 6, *F3, nullptr, 0.0, s));
@@ -380,6 +418,48 @@ extern "C" int hp_pendulum_propagate(hp_plan* p, const double* Fold, double* Fne
   HP_CHECK(hp_full_to_internal(p, dF, b0, p->stream));
   double2 *F = b0, *F2 = b1, *F3 = b2;
   HP_CHECK(integrate_internal(p, &F, &F2, &F3, ac, dt, method));
+  double2* dOut = (double2*)stage_out(p, "api.Fout", Fnew, fb, mem, &st);
+  if (st) return st;
+  HP_CHECK(hp_internal_to_full(p, F, dOut, p->stream));
+  HP_CHECK(finish_out(p, Fnew, dOut, fb, mem));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
+extern "C" int hp_pendulum_propagate_den(hp_plan* p, const double* Fold, const double* f, double* Fnew,
+                                         double dt, int method, int mem) {
+  if (!p || !Fold || !Fnew) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  HP_CHECK(check_mem(mem));
+  if (!p->has_model || !p->den_mR) { hp_set_error("no density-gravity model: call hp_plan_set_den_model first"); return HP_ERR_NO_MODEL; }
+  if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
+  if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
+  int st = HP_OK;
+  const void* fg = nullptr;
+  if (f) {
+    const long long ng = p->n_grid();
+    const double* df = (const double*)stage_in(p, "api.fin", f, sizeof(double) * ng, mem, &st);
+    if (st) return st;
+    fg = df;
+    if (p->precision == HP_MIXED) {
+      float* t = (float*)p->ws_get("api.f32", sizeof(float) * ng, &st);
+      if (st) return st;
+      ProfScope _ps(p, "convert", p->stream);
+      k_d2f<<<(unsigned)((ng + 255) / 256), 256, 0, p->stream>>>(df, t, ng);
+      HP_CUDA_TRY(cudaGetLastError());
+      fg = t;
+    }
+  }
+  const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
+  const double2* dF = (const double2*)stage_in(p, "api.Fin", Fold, fb, mem, &st);
+  if (st) return st;
+  double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
+  double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
+  double2* b2 = (method == HP_EULER) ? nullptr : (double2*)p->ws_get("api.S2", ib, &st); if (st) return st;
+  double2* ac = (method == HP_RK2 || method == HP_RK4) ? (double2*)p->ws_get("api.S3", ib, &st) : nullptr;
+  if (st) return st;
+  HP_CHECK(hp_full_to_internal(p, dF, b0, p->stream));
+  double2 *F = b0, *F2 = b1, *F3 = b2;
+  HP_CHECK(integrate_internal(p, &F, &F2, &F3, ac, dt, method, fg));
   double2* dOut = (double2*)stage_out(p, "api.Fout", Fnew, fb, mem, &st);
   if (st) return st;
   HP_CHECK(hp_internal_to_full(p, F, dOut, p->stream));
@@ -445,7 +525,7 @@ extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
 
 extern "C" int hp_state_destroy(hp_state* s) {
   if (!s) return HP_OK;
-  cudaFree(s->F); cudaFree(s->F2); cudaFree(s->F3); cudaFree(s->acc);
+  cudaFree(s->F); cudaFree(s->F2); cudaFree(s->F3); cudaFree(s->acc); cudaFree(s->fg);
   delete s;
   return HP_OK;
 }
@@ -459,6 +539,7 @@ extern "C" int hp_state_load(hp_state* s, const double* F, int mem) {
   if (st) return st;
   HP_CHECK(hp_full_to_internal(p, d, s->F, p->stream));
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  s->fg_valid = false;
   return HP_OK;
 }
 
@@ -480,13 +561,52 @@ extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
   if (!s || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
   hp_plan* p = s->plan;
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (nsteps > 0) s->fg_valid = false;
   for (int k = 0; k < nsteps; ++k) HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
   return HP_OK;
 }
 
+// pendulum_reduced_hybrid.m:226-234 per step: F = propagate_den(F, f);
+// f = backward(F); f += dt * df(f); F = forward(f).
+extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int method, int nsteps) {
+  if (!s || !c || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  hp_plan* p = s->plan;
+  if (hp_collision_plan(c) != p) { hp_set_error("collision operator belongs to another plan"); return HP_ERR_INVALID; }
+  if (!p->has_model || !p->den_mR) { hp_set_error("no density-gravity model: call hp_plan_set_den_model first"); return HP_ERR_NO_MODEL; }
+  if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
+  if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
+  cudaStream_t st = p->stream;
+  if (!s->fg) {
+    const size_t eb = p->precision == HP_FP64 ? sizeof(double) : sizeof(float);
+    if (cudaMalloc(&s->fg, eb * (size_t)p->n_grid()) != cudaSuccess) {
+      cudaGetLastError();
+      s->fg = nullptr;
+      hp_set_error("device allocation failed");
+      return HP_ERR_ALLOC;
+    }
+  }
+  if (!s->fg_valid && nsteps > 0) HP_CHECK(hp_backward_internal(p, s->F, s->fg, 0, st));
+  for (int k = 0; k < nsteps; ++k) {
+    s->fg_valid = false;
+    HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method, s->fg));
+    HP_CHECK(hp_backward_internal(p, s->F, s->fg, 0, st));
+    HP_CHECK(hp_collision_apply(c, s->fg, dt, st));
+    HP_CHECK(hp_forward_internal(p, s->fg, 0, s->F, st));
+    s->fg_valid = true;
+  }
+  return HP_OK;
+}
+
+// The grid density of the state: after hybrid steps the post-collision
+// density (the f of pendulum_reduced_hybrid.m:233), else backward(F).
 extern "C" int hp_state_density(hp_state* s, void* f) {
   if (!s || !f) { hp_set_error("null argument"); return HP_ERR_INVALID; }
   hp_plan* p = s->plan;
+  if (s->fg_valid) {
+    const size_t eb = p->precision == HP_FP64 ? sizeof(double) : sizeof(float);
+    HP_CUDA_TRY(cudaMemcpyAsync(f, s->fg, eb * (size_t)p->n_grid(), cudaMemcpyDeviceToDevice, p->stream));
+    return HP_OK;
+  }
   return hp_backward_internal(p, s->F, f, p->symmetry == HP_COMPLEX, p->stream);
 }
 
@@ -503,6 +623,7 @@ extern "C" int hp_state_normalize(hp_state* s, double mass, double* scale) {
   hp_plan* p = s->plan;
   const double f = mass / m0;
   const long long n = p->nrows * p->nx;
+  s->fg_valid = false;
   {
     ProfScope _ps(p, "normalize", p->stream);
     k_scale_c64<<<(unsigned)((n + 255) / 256), 256, 0, p->stream>>>(s->F, n, f);

@@ -157,6 +157,32 @@ __global__ void k_coll_df(int nx, int nR, int numR, int nD, const int* __restric
   df[(long long)ix * nR + iR] = (T)(s - lambda[t] * (double)f[(long long)ix * nR + iR]);
 }
 
+// f += dt * df(f) in place (pendulum_reduced_hybrid.m:232-233): the colliding
+// columns are first gathered into fk[ix][k] so that every tap reads the
+// pre-update density.
+template <typename T>
+__global__ void k_coll_gather(int nx, int nR, int numR, const int* __restrict__ indR, const T* __restrict__ f,
+                              T* __restrict__ fk) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * numR) return;
+  const int k = (int)(t % numR), ix = (int)(t / numR);
+  fk[t] = f[(long long)ix * nR + indR[k]];
+}
+
+template <typename T>
+__global__ void k_coll_update(int nx, int nR, int numR, int nD, const int* __restrict__ indR,
+                              const double* __restrict__ lambda, const double* __restrict__ fcL,
+                              const short* __restrict__ idx, const T* __restrict__ fk, T* __restrict__ f,
+                              double dt) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * numR) return;
+  const int k = (int)(t % numR), ix = (int)(t / numR);
+  double s = 0.0;
+  for (int d = 0; d < nD; ++d) s += fcL[t * nD + d] * (double)fk[(long long)idx[t * nD + d] * numR + k];
+  const double f0 = (double)fk[t];
+  f[(long long)ix * nR + indR[k]] = (T)(f0 + dt * (s - lambda[t] * f0));
+}
+
 // --------------------------------------------------------------- C ABI ----
 struct hp_collision {
   hp_plan* plan = nullptr;
@@ -304,3 +330,26 @@ extern "C" int hp_collision_df(hp_collision* c, const double* f, double* df, int
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HP_OK;
 }
+
+template <typename T>
+static int coll_apply_T(hp_collision* c, T* f, double dt, cudaStream_t s) {
+  hp_plan* p = c->plan;
+  if (c->t.numR == 0) return HP_OK;
+  const long long nR = 8LL * p->B * p->B * p->B, nx = (long long)p->N * p->N, nt = nx * c->t.numR;
+  int st = HP_OK;
+  T* fk = (T*)p->ws_get("coll.fk", sizeof(T) * nt, &st);
+  if (st) return st;
+  ProfScope _ps(p, "coll.df", s);
+  k_coll_gather<T><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>((int)nx, (int)nR, c->t.numR, c->t.indR, f, fk);
+  k_coll_update<T><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>((int)nx, (int)nR, c->t.numR, c->t.nD, c->t.indR,
+                                                                c->t.lambda, c->t.fcL, c->t.idx, fk, f, dt);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+int hp_collision_apply(hp_collision* c, void* f, double dt, cudaStream_t s) {
+  if (c->plan->precision == HP_FP64) return coll_apply_T<double>(c, (double*)f, dt, s);
+  return coll_apply_T<float>(c, (float*)f, dt, s);
+}
+
+hp_plan* hp_collision_plan(const hp_collision* c) { return c->plan; }

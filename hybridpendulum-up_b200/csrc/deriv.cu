@@ -27,6 +27,12 @@
 
 using namespace hp;
 
+#define HP_CHECK_RET(expr)          \
+  do {                              \
+    int _s = (expr);                \
+    if (_s != HP_OK) return _s;     \
+  } while (0)
+
 struct DerivParams {
   double L;
   double b[3];
@@ -167,6 +173,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
                                                   const double2* __restrict__ Fev,
                                                   const c2<T>* __restrict__ P3,
                                                   const c2<T>* __restrict__ Gl,
+                                                  const c2<T>* __restrict__ Gx,
                                                   const double2* __restrict__ F0, double a,
                                                   double2* __restrict__ out,
                                                   double2* __restrict__ acc, double bacc,
@@ -391,6 +398,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
           const int c = e / (N * N), q = e % (N * N);
           gi[u] = row_of(L, tl.l, tl.m, tl.n0 + c) * L.nx + pbase + q;
           g[u] = Gl[gi[u]];
+          if (Gx) g[u] = g[u] + Gx[gi[u]];
           f0[u] = F0 ? F0[gi[u]] : make_double2(0.0, 0.0);
           if (acc) ac[u] = acc[gi[u]];
         }
@@ -426,7 +434,7 @@ template <typename T> static size_t plane_smem(int N, bool p3) {
 
 template <int N, typename T>
 static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                       double2* acc, double bacc, cudaStream_t s, const DerivParams& prm) {
+                       double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
   using C = c2<T>;
   int st = HP_OK;
   const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
@@ -478,10 +486,10 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   ProfScope _ps(p, "deriv.plane", s);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, (const C*)Gx, F0, a, out, acc, bacc, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, (const C*)Gx, F0, a, out, acc, bacc, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -489,25 +497,74 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
 
 template <typename T>
 static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                     double2* acc, double bacc, cudaStream_t s, const DerivParams& prm) {
+                     double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
   switch (p->N) {
-    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
-    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm);
+    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     default:
       hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
       return HP_ERR_UNSUPPORTED;
   }
 }
 
+// Density-side gravity of pendulum_reduced_den.m:449-516:
+// Gx = -sum_i D_i fftSO3R(f . mR_i), with f the given grid density (first
+// stage) or the backward transform of Feval (later stages, :454-475).
+template <typename T>
+__global__ void k_den_combine(const c2<T>* __restrict__ FMR, c2<T>* __restrict__ Gx, long long nrows, long long nx,
+                              int N, int axis, double tp, int first) {
+  using C = c2<T>;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= nrows * nx) return;
+  const long long w = t % nx;
+  const int k = (int)((axis == 0 ? w : w / N) % N);
+  const T dk = (T)(tp * kappa_first(k, N));
+  const C v = FMR[t];
+  C g;                               // -(i dk) v
+  g.x = dk * v.y;
+  g.y = -dk * v.x;
+  Gx[t] = first ? g : Gx[t] + g;
+}
+
+template <typename T>
+static int den_gravity(hp_plan* p, const double2* Fev, const void* fgrid, cudaStream_t s, c2<T>** Gx_out) {
+  using C = c2<T>;
+  int st = HP_OK;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  C* Gx = (C*)p->ws_get("deriv.Gden", fb, &st);
+  if (st) return st;
+  C* FMR = (C*)p->ws_get("deriv.FMR", fb, &st);
+  if (st) return st;
+  const void* f = fgrid;
+  if (!f) {
+    T* fg = (T*)p->ws_get("deriv.fden", sizeof(T) * (size_t)p->n_grid(), &st);
+    if (st) return st;
+    HP_CHECK_RET(hp_backward_internal(p, Fev, fg, 0, s));
+    f = fg;
+  }
+  for (int i = 0; i < 2; ++i) {
+    HP_CHECK_RET(hp_forward_internal_T(p, f, p->den_mR + (size_t)i * 8 * p->B * p->B * p->B, FMR, s));
+    const long long n = p->nrows * p->nx;
+    ProfScope _ps(p, "deriv.den", s);
+    k_den_combine<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(FMR, Gx, p->nrows, p->nx, p->N, i,
+                                                              2.0 * M_PI / p->model.L, i == 0);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  *Gx_out = Gx;
+  return HP_OK;
+}
+
 // out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
+// With a density-gravity model (hp_pendulum_propagate_den), fgrid is the grid
+// density of Feval when the caller has it (else it is recomputed from Feval).
 int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                       double2* acc, double bacc, cudaStream_t s) {
+                       double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   DerivParams prm;
@@ -515,8 +572,14 @@ int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double
   for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; }
   for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
   if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
-  if (p->precision == HP_FP64) return run_deriv<double>(p, Fev, F0, a, out, acc, bacc, s, prm);
-  return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm);
+  if (p->precision == HP_FP64) {
+    double2* Gx = nullptr;
+    if (p->den_mR) HP_CHECK_RET(den_gravity<double>(p, Fev, fgrid, s, &Gx));
+    return run_deriv<double>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+  }
+  float2* Gx = nullptr;
+  if (p->den_mR) HP_CHECK_RET(den_gravity<float>(p, Fev, fgrid, s, &Gx));
+  return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
 }
 
 // ------------------------------------------ derivative without allocation ----
@@ -609,10 +672,10 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   dim3 grid((unsigned)ntiles, p3 ? N : 1);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return hp_internal_to_full(p, dFi, dFfull, s);

@@ -59,6 +59,7 @@ struct hp_plan {
   int* tap_row = nullptr;    // [row][9] source rows of the non-zero taps
   int* tap_cnt = nullptr;    // [row] number of non-zero taps
   double2* tap_w = nullptr;  // [row][9][3] weights per component
+  double* den_mR = nullptr;  // [2][(2B)^3] density-side gravity multipliers (pendulum_reduced_den)
 
   // profiling
   bool prof_on = false;
@@ -86,7 +87,14 @@ struct hp_state {
   double2* F2 = nullptr;    // ping-pong / stage buffers
   double2* F3 = nullptr;
   double2* acc = nullptr;
+  void* fg = nullptr;       // grid density of the hybrid step (compute precision)
+  bool fg_valid = false;    // fg holds the post-collision density of F
 };
+
+struct hp_collision;
+// f += dt * df(f), in place, f in the plan's compute precision (device).
+int hp_collision_apply(hp_collision* c, void* f, double dt, cudaStream_t s);
+hp_plan* hp_collision_plan(const hp_collision* c);
 
 // <l1 m1; 1 m2 | l m> with m1 = m - m2, l = l1 + dl (dl in -1..1):
 // cg1[((l1 * 3 + (dl+1)) * (2*lmax+3) + (m + lmax+1)) * 3 + (m2+1)]
@@ -112,7 +120,11 @@ int hp_build_gravity_taps(hp_plan* p, const double2* MR_full_dev);
 int hp_full_to_internal(hp_plan* p, const double2* Ffull, double2* Fint, cudaStream_t s);
 int hp_internal_to_full(hp_plan* p, const double2* Fint, double2* Ffull, cudaStream_t s);
 int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, double a,
-                       double2* out, double2* acc, double bacc, cudaStream_t s);
+                       double2* out, double2* acc, double bacc, cudaStream_t s,
+                       const void* fgrid = nullptr);
+// Forward transform of mult . f (mult: (2B)^3 grid samples, may be null) into
+// [row][omega] coefficients in the plan's compute precision (c2<T>).
+int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* out, cudaStream_t s);
 int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s);
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s);
 int hp_prod_launch(hp_plan* p, const double2* F, const double2* G, double2* FG, int batch,

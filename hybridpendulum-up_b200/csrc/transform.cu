@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
 template <int B, typename T, int NB, bool CPLX>
 __global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restrict__ fin,
                                               const T* __restrict__ wig, const double* __restrict__ qw,
+                                              const double* __restrict__ mult,
                                               c2<T>* __restrict__ Fa, int P, long long w_per_block) {
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
@@ -317,6 +318,11 @@ __global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restric
       C v;
       if (CPLX) v = reinterpret_cast<const C*>(fin)[gi];
       else { v.x = reinterpret_cast<const T*>(fin)[gi]; v.y = 0; }
+      if (mult) {  // pointwise multiplier on the rotation grid (index a + 2B b + 4B^2 c)
+        const T mv = (T)mult[a + NB2 * ((b0 + bq) + NB2 * cc)];
+        v.x *= mv;
+        v.y *= mv;
+      }
       sIn[(((size_t)pp * NB + bq) * NB2 + cc) * NB2 + a] = v;
     }
     __syncthreads();
@@ -485,7 +491,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
 }
 
 template <int B, typename T, bool CPLX>
-static int anal_launch(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
+static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
   using C = c2<T>;
   constexpr int NB = TfCfg<T>::NB, NB2 = 2 * B;
   constexpr int NM = CPLX ? 2 * B - 1 : B;
@@ -512,7 +518,7 @@ static int anal_launch(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
   k_anal<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), f,
                                                       p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
                                                                               : (const T*)(const void*)p->wig32,
-                                                      p->qw, Fa, P, wpb);
+                                                      p->qw, mult, Fa, P, wpb);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
@@ -532,9 +538,9 @@ static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
 }
 
 template <typename T, bool CPLX>
-static int anal_any(hp_plan* p, const void* f, c2<T>* Fa, cudaStream_t s) {
+static int anal_any(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
   switch (p->B) {
-#define X(b) case b: return anal_launch<b, T, CPLX>(p, f, Fa, s);
+#define X(b) case b: return anal_launch<b, T, CPLX>(p, f, mult, Fa, s);
     HP_FOR_EACH_B(X)
 #undef X
     default:
@@ -556,8 +562,10 @@ static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out,
   return synth_any<T, false>(p, t1, f, s);
 }
 
+// Forward transform of (mult .) f into [row][omega] coefficients of type c2<T>.
 template <typename T>
-static int forward_T(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {
+static int forward_rows_T(hp_plan* p, const void* f, int complex_in, const double* mult, c2<T>* out,
+                          cudaStream_t s) {
   using C = c2<T>;
   int st = HP_OK;
   const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
@@ -565,18 +573,27 @@ static int forward_T(hp_plan* p, const void* f, int complex_in, double2* Fint, c
   if (st) return st;
   C* t2 = (C*)p->ws_get("tf.t2", fb, &st);
   if (st) return st;
-  st = complex_in ? anal_any<T, true>(p, f, t1, s) : anal_any<T, false>(p, f, t1, s);
+  st = complex_in ? anal_any<T, true>(p, f, mult, t1, s) : anal_any<T, false>(p, f, mult, t1, s);
   if (st) return st;
   dim3 grid((unsigned)((p->nrows + 31) / 32), (unsigned)((p->nx + 31) / 32));
   { ProfScope _ps(p, "tf.transpose", s);
   k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nx, p->nrows); }
   HP_CUDA_TRY(cudaGetLastError());
-  st = omega_fft_any<T, T>(p, t2, t1, false, s);
+  return omega_fft_any<T, T>(p, t2, out, false, s);
+}
+
+template <typename T>
+static int forward_T(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {
+  using C = c2<T>;
+  int st = HP_OK;
+  C* t3 = (C*)p->ws_get("tf.t1", sizeof(C) * (size_t)p->nrows * p->nx, &st);  // free again after the transpose
+  if (st) return st;
+  st = forward_rows_T<T>(p, f, complex_in, nullptr, t3, s);
   if (st) return st;
   // to FP64 rows
   const long long n = p->nrows * p->nx;
   ProfScope _ps(p, "convert", s);
-  k_to_c64<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(t1, Fint, n);
+  k_to_c64<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(t3, Fint, n);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
@@ -591,4 +608,11 @@ int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   if (p->precision == HP_FP64) return forward_T<double>(p, f, complex_in, Fint, s);
   return forward_T<float>(p, f, complex_in, Fint, s);
+}
+
+int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* out, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  const int cplx = p->symmetry == HP_COMPLEX;
+  if (p->precision == HP_FP64) return forward_rows_T<double>(p, f, cplx, mult, (double2*)out, s);
+  return forward_rows_T<float>(p, f, cplx, mult, (float2*)out, s);
 }

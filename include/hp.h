@@ -132,6 +132,23 @@ int hp_pendulum_propagate(hp_plan* plan, const double* Fold, double* Fnew, doubl
 /* The derivative dF of pendulum.m:388-527 / pendulum_reduced.m:362-465. */
 int hp_pendulum_derivative(hp_plan* plan, const double* F, double* dF, int mem);
 
+/* Density-side gravity model of the reduced pendulum: the inputs of the MEX
+ * pendulum_propagate_reduced_den(F,f,X,mR,bt,G,dt,L,u,d,w,method)
+ * (propagation/mex/sources/pendulum_propagate_reduced_den/kernel.cu:9-325,
+ * integrate.cu:220-445) and of pendulum_reduced_den.m:401-533.  The gravity
+ * term is formed on the grid, FMR_i = fftSO3R(f . mR_i), instead of by the
+ * Clebsch-Gordan product.  model: L, b, G as for hp_plan_set_model (gyro
+ * unused).  mR: real (2, 2B, 2B, 2B), component fastest (MATLAB layout of
+ * pendulum_reduced_den.m:132).  Needs ndim = 2 and HP_REAL; replaces any model
+ * set by hp_plan_set_model (and is replaced by it). */
+int hp_plan_set_den_model(hp_plan* plan, const hp_model* model, const double* mR, int mem);
+/* One step of the density-gravity model.  f: the real grid density of Fold,
+ * (2B,2B,2B,2Bx,2Bx), used by the first derivative evaluation; NULL recomputes
+ * it from Fold by the backward transform (the later stages always do so, as
+ * integrate.cu of the reference MEX and pendulum_reduced_den.m:359-399). */
+int hp_pendulum_propagate_den(hp_plan* plan, const double* Fold, const double* f, double* Fnew,
+                              double dt, int method, int mem);
+
 /* Derivative without allocation: the same dF as hp_pendulum_derivative, for
  * callers that must not allocate device memory while they run (a propagation
  * loop on a GPU whose memory another framework owns through its own allocator,
@@ -196,8 +213,16 @@ int hp_state_load(hp_state* state, const double* F, int mem);   /* full layout i
 int hp_state_store(hp_state* state, double* F, int mem);        /* full layout out */
 /* nsteps steps of `method` with step dt. */
 int hp_state_step(hp_state* state, double dt, int method, int nsteps);
-/* Density on the grid f = ifftSO3R(F) of the current state into `f`
- * (device pointer; double for HP_FP64 plans, float for HP_MIXED plans). */
+/* nsteps hybrid steps of pendulum_reduced_hybrid.m:224-234, each
+ *   F = propagate_den(F, f); f = fftSO3R backward(F); f += dt*df(f); F = forward(f)
+ * with df the collision operator of `coll` (pendulum_reduced_discrete_propagate,
+ * propagation/discrete/mex/sources/pendulum_reduced_collision/propagate.cu:6-121).
+ * The plan needs hp_plan_set_den_model; coll must be created on the same plan.
+ * The grid density f stays on the device between steps (compute precision). */
+int hp_state_hybrid_step(hp_state* state, hp_collision* coll, double dt, int method, int nsteps);
+/* Density on the grid of the current state into `f` (device pointer; double
+ * for HP_FP64 plans, float for HP_MIXED plans): after hybrid steps the
+ * post-collision density f of the last step, otherwise f = ifftSO3R(F). */
 int hp_state_density(hp_state* state, void* f);
 /* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
 int hp_state_mass(hp_state* state, double* mass);
