@@ -41,7 +41,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_state_mass', 'hp_plan_profile', 'hp_plan_profile_get', 'hp_plan_launch_count',
            'hp_pendulum_derivative_noalloc', 'hp_state_normalize', 'hp_collision_create',
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
-           'hp_pendulum_propagate_den', 'hp_state_hybrid_step']
+           'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
+           'hp_pendulum_adjoint']
 
 
 class HPError(RuntimeError):
@@ -53,6 +54,11 @@ class HPError(RuntimeError):
 class hp_model(ctypes.Structure):
     _fields_ = [('L', ctypes.c_double), ('b', ctypes.c_double * 3), ('G', ctypes.c_double * 9),
                 ('gyro', ctypes.c_double * 3)]
+
+
+class hp_model_grad(ctypes.Structure):
+    _fields_ = [('b', ctypes.c_double * 3), ('G', ctypes.c_double * 9), ('gyro', ctypes.c_double * 3),
+                ('gscale', ctypes.c_double * 3)]
 
 
 class hp_collision_params(ctypes.Structure):
@@ -96,6 +102,8 @@ def _load():
         'hp_plan_set_den_model': [vp, ctypes.POINTER(hp_model), vp, ip],
         'hp_pendulum_propagate_den': [vp, vp, vp, vp, dp, ip, ip],
         'hp_state_hybrid_step': [vp, vp, dp, ip, ip],
+        'hp_pendulum_derivative_adjoint': [vp, vp, vp, ip],
+        'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -300,6 +308,35 @@ class Plan:
         _check(_lib.hp_pendulum_propagate_den(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(pf),
                                               ctypes.c_void_p(po), float(dt), METHODS[method.lower()], mi))
         return out
+
+    def derivative_adjoint(self, lam, out=None):
+        """A^H lam, the adjoint of ``derivative`` under <X, Y> = Re sum conj(X) Y."""
+        lam = _as_matlab(lam, np.complex128)
+        if out is None:
+            out = _empty_like_mem(lam, self.F_shape, np.complex128)
+        pi, mi = _ptr(lam, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        _check(_lib.hp_pendulum_derivative_adjoint(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), mi))
+        return out
+
+    def adjoint(self, F0, lamT, nsteps: int, dt: float, checkpoint_every: int = 10, method: str = 'euler'):
+        """Reverse pass of ``nsteps`` Euler steps from F0 for a loss with gradient
+        lamT at F_T.  Returns (lam0, grads) with grads = dict(b, G, gyro, gscale)."""
+        F0 = _as_matlab(F0, np.complex128)
+        lamT = _as_matlab(lamT, np.complex128)
+        lam0 = _empty_like_mem(F0, self.F_shape, np.complex128)
+        pf, mf = _ptr(F0, np.complex128)
+        pl, ml = _ptr(lamT, np.complex128)
+        po, _ = _ptr(lam0, np.complex128)
+        if mf != ml:
+            raise ValueError('F0 and lamT must live in the same memory space')
+        g = hp_model_grad()
+        _check(_lib.hp_pendulum_adjoint(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(pl), int(nsteps), float(dt),
+                                        METHODS[method.lower()], int(checkpoint_every), ctypes.c_void_p(po),
+                                        ctypes.byref(g), mf))
+        grads = dict(b=np.array(g.b[:]), G=np.array(g.G[:]).reshape(3, 3), gyro=np.array(g.gyro[:]),
+                     gscale=np.array(g.gscale[:]))
+        return lam0, grads
 
     def derivative(self, F, out=None):
         F = _as_matlab(F, np.complex128)

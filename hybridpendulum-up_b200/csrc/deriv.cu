@@ -33,12 +33,6 @@ using namespace hp;
     if (_s != HP_OK) return _s;     \
   } while (0)
 
-struct DerivParams {
-  double L;
-  double b[3];
-  double G[9];
-  double gyro[3];
-};
 
 // -------------------------------------------------------- pass A: axis 3 ----
 template <int N, typename T>
@@ -117,6 +111,9 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
       dd[a] = tp * (T)kappa_diag(k, N);
     }
   }
+  T d1g[NDIM];  // D_i times the gravity scale of component i
+#pragma unroll
+  for (int a = 0; a < NDIM; ++a) d1g[a] = d1[a] * (T)prm.gs[a];
   T noise = 0;
 #pragma unroll
   for (int i = 0; i < NDIM; ++i)
@@ -135,8 +132,8 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
 #pragma unroll
       for (int i = 0; i < NDIM; ++i) {
         const double2 wv = tap_w[(rg * 9 + t) * 3 + i];
-        cx += d1[i] * (T)wv.y;
-        cy -= d1[i] * (T)wv.x;
+        cx += d1g[i] * (T)wv.y;
+        cy -= d1g[i] * (T)wv.x;
       }
       const C fs = tile[(src - r0) * W + w];
       ax += cx * fs.x - cy * fs.y;
@@ -291,7 +288,8 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
     const C* fp = sF + (c + 2) * PS;
     const C* pp = sP + c * PS;
     const int n = tl.n0 + c, l = tl.l;
-    const T ap = sqrt((T)((l - n) * (l + n + 1))), am = sqrt((T)((l + n) * (l - n + 1)));
+    const T lie = (T)prm.lie;
+    const T ap = lie * sqrt((T)((l - n) * (l + n + 1))), am = lie * sqrt((T)((l + n) * (l - n + 1)));
     C x[N];
     if (kind == 0) {
       // Y0 = a+ F~+ (0.5i x1 - 0.5 x2) + a- F~- (0.5i x1 + 0.5 x2) - g3 D3 x1 x2 F~ + (i n + b3 D3) P~
@@ -312,7 +310,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
           y.x += s * v0.y;
           y.y -= s * v0.x;
           // (i n + b3 i d3) pv = i (n + b3 d3) pv
-          const T q = (T)n + b3 * d3;
+          const T q = lie * (T)n + b3 * d3;
           y.x -= q * pv.y;
           y.y += q * pv.x;
         }
@@ -563,23 +561,37 @@ static int den_gravity(hp_plan* p, const double2* Fev, const void* fgrid, cudaSt
 // out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
 // With a density-gravity model (hp_pendulum_propagate_den), fgrid is the grid
 // density of Feval when the caller has it (else it is recomputed from Feval).
-int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                       double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
-  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
-  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+DerivParams hp_model_params(const hp_plan* p) {
   DerivParams prm;
   prm.L = p->model.L;
-  for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; }
+  for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; prm.gs[i] = 1.0; }
   for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
+  prm.lie = 1.0;
   if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
+  return prm;
+}
+
+int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Fev, const double2* F0, double a,
+                           double2* out, double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  const bool den = p->den_mR != nullptr && (prm.gs[0] != 0 || prm.gs[1] != 0);
   if (p->precision == HP_FP64) {
     double2* Gx = nullptr;
-    if (p->den_mR) HP_CHECK_RET(den_gravity<double>(p, Fev, fgrid, s, &Gx));
+    if (den) HP_CHECK_RET(den_gravity<double>(p, Fev, fgrid, s, &Gx));
     return run_deriv<double>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
   }
   float2* Gx = nullptr;
-  if (p->den_mR) HP_CHECK_RET(den_gravity<float>(p, Fev, fgrid, s, &Gx));
+  if (den) HP_CHECK_RET(den_gravity<float>(p, Fev, fgrid, s, &Gx));
   return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+}
+
+// out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
+// With a density-gravity model (hp_pendulum_propagate_den), fgrid is the grid
+// density of Feval when the caller has it (else it is recomputed from Feval).
+int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
+                       double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
+  return hp_derivative_eval_prm(p, hp_model_params(p), Fev, F0, a, out, acc, bacc, s, fgrid);
 }
 
 // ------------------------------------------ derivative without allocation ----
@@ -705,11 +717,11 @@ extern "C" int hp_pendulum_derivative_noalloc(hp_plan* p, const double* F, doubl
   void* base = nullptr;
   int st = noalloc_scratch(&base);
   if (st) return st;
-  DerivParams prm;
-  prm.L = p->model.L;
-  for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; }
-  for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
-  if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
+  if (p->den_mR) {
+    hp_set_error("the allocation-free derivative does not cover density-gravity models");
+    return HP_ERR_UNSUPPORTED;
+  }
+  const DerivParams prm = hp_model_params(p);
   const double2* Fin = reinterpret_cast<const double2*>(F);
   double2* out = reinterpret_cast<double2*>(dF);
   unsigned char* b = static_cast<unsigned char*>(base);

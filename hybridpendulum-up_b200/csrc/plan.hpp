@@ -119,6 +119,21 @@ int hp_twiddles_init();
 int hp_build_gravity_taps(hp_plan* p, const double2* MR_full_dev);
 int hp_full_to_internal(hp_plan* p, const double2* Ffull, double2* Fint, cudaStream_t s);
 int hp_internal_to_full(hp_plan* p, const double2* Fint, double2* Ffull, cudaStream_t s);
+// Coefficients of the derivative terms: lie scales the Lie (u) term, gs[i]
+// the gravity component i (coefficient taps, or the density-side term of a
+// density-gravity model when gs[0] or gs[1] is non-zero); b, G, gyro as in hp_model.
+struct DerivParams {
+  double L;
+  double b[3];
+  double G[9];
+  double gyro[3];
+  double lie;
+  double gs[3];
+};
+DerivParams hp_model_params(const hp_plan* p);
+int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Feval, const double2* F0,
+                           double a, double2* out, double2* acc, double bacc, cudaStream_t s,
+                           const void* fgrid = nullptr);
 int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, double a,
                        double2* out, double2* acc, double bacc, cudaStream_t s,
                        const void* fgrid = nullptr);

@@ -149,6 +149,27 @@ int hp_plan_set_den_model(hp_plan* plan, const hp_model* model, const double* mR
 int hp_pendulum_propagate_den(hp_plan* plan, const double* Fold, const double* f, double* Fnew,
                               double dt, int method, int mem);
 
+/* ---- reverse mode (no counterpart in the reference) ----
+ * Gradients of a scalar loss L(F_T) of a forward-Euler trajectory
+ * F_{n+1} = F_n + dt A F_n (hp_pendulum_propagate with HP_EULER), with the
+ * convention dL = Re sum conj(lam) dF over the full layout (the convention of
+ * torch complex gradients).  For HP_REAL plans gradients are those on the
+ * real-density subspace: lamT is first projected onto it and lam0 lies in it. */
+typedef struct {
+  double b[3];       /* dL/db_i                                                */
+  double G[9];       /* dL/dG_ij (row-major; G_ij and G_ji enter through one term) */
+  double gyro[3];    /* dL/dgyro_i (ndim = 3)                                  */
+  double gscale[3];  /* dL/ds_i at s = 1, where MR_i -> s_i MR_i (a J_i^-1 scale) */
+} hp_model_grad;
+/* out = A^H lam (the exact adjoint of hp_pendulum_derivative), full layout. */
+int hp_pendulum_derivative_adjoint(hp_plan* plan, const double* lam, double* out, int mem);
+/* Reverse pass of nsteps Euler steps from F0: lam0 = dL/dF0 and the model
+ * gradients.  The trajectory is recomputed from checkpoints taken every
+ * checkpoint_every steps (device memory: ceil(nsteps/k) + k states).
+ * method must be HP_EULER; lam0 or grad may be NULL. */
+int hp_pendulum_adjoint(hp_plan* plan, const double* F0, const double* lamT, int nsteps, double dt,
+                        int method, int checkpoint_every, double* lam0, hp_model_grad* grad, int mem);
+
 /* Derivative without allocation: the same dF as hp_pendulum_derivative, for
  * callers that must not allocate device memory while they run (a propagation
  * loop on a GPU whose memory another framework owns through its own allocator,
