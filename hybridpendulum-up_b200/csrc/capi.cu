@@ -154,7 +154,7 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
 extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
   cudaFree(p->rows); cudaFree(p->seg); cudaFree(p->wig64); cudaFree(p->wig32); cudaFree(p->wfull);
-  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_row); cudaFree(p->tap_cnt); cudaFree(p->tap_w);
+  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_wr); cudaFree(p->tap_wr32);
   p->prof_on = false;
   prof_collect(p);
   for (auto& kv : p->ws) cudaFree(kv.second.p);
@@ -231,11 +231,12 @@ extern "C" int hp_plan_set_model(hp_plan* p, const hp_model* m, const double* MR
     hp_set_error("MR has components outside the degree-1, m2=0 block (alpha-dependent multiplier)");
     return HP_ERR_UNSUPPORTED;
   }
-  int st = HP_OK;
-  double2* dMR = (double2*)p->ws_get("model.MR", sizeof(double2) * nMR, &st);
-  if (st) return st;
-  HP_CUDA_TRY(cudaMemcpy(dMR, h.data(), sizeof(double2) * nMR, cudaMemcpyHostToDevice));
-  HP_CHECK(hp_build_gravity_taps(p, dMR));
+  HP_CHECK(hp_build_gravity_taps(p));
+  for (int n2 = -1; n2 <= 1; ++n2)
+    for (int i = 0; i < 3; ++i)
+      p->mr1[n2 + 1][i] = (i < p->ndim && lmax >= 1)
+                              ? h[lmax + (size_t)D * (n2 + lmax) + (size_t)D * D * 1 + (size_t)D * D * (lmax + 1) * i]
+                              : make_double2(0.0, 0.0);
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   p->model = *m;
   p->den_mR = nullptr;
@@ -265,11 +266,9 @@ extern "C" int hp_plan_set_den_model(hp_plan* p, const hp_model* m, const double
   double* d = (double*)p->ws_get("model.denmR", sizeof(double) * 2 * ng, &st);
   if (st) return st;
   HP_CUDA_TRY(cudaMemcpy(d, dein.data(), sizeof(double) * 2 * ng, cudaMemcpyHostToDevice));
-  const size_t nMR = (size_t)p->D * p->D * (p->lmax + 1) * p->ndim;
-  double2* dMR = (double2*)p->ws_get("model.MR", sizeof(double2) * nMR, &st);
-  if (st) return st;
-  HP_CUDA_TRY(cudaMemsetAsync(dMR, 0, sizeof(double2) * nMR, p->stream));
-  HP_CHECK(hp_build_gravity_taps(p, dMR));  // no coefficient-space gravity
+  HP_CHECK(hp_build_gravity_taps(p));
+  for (int n2 = 0; n2 < 3; ++n2)
+    for (int i = 0; i < 3; ++i) p->mr1[n2][i] = make_double2(0.0, 0.0);  // no coefficient-space gravity
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   p->model = *m;
   p->den_mR = d;

@@ -60,40 +60,52 @@ __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __res
 }
 
 // ------------------------------------------------ pass B: gravity + noise ----
-// Block = one m group x W consecutive omega points.  The group's rows are
-// staged once in shared memory (taps stay inside the group because the gravity
-// multiplier has m2 = 0); a warp handles one output row at a time, lanes are
-// omega points, so tap metadata is warp-uniform and global accesses coalesced.
+// Block = one m group x W consecutive omega points.  The group's rows and
+// their real tap weights are staged once in shared memory (taps stay inside
+// the group because the gravity multiplier has m2 = 0); a warp handles one
+// output row at a time, lanes are omega points, so the tap loop is
+// warp-uniform and reads shared memory only.  Per omega point the model part
+// of the weights folds into nu[n2] = -i sum_i D_i gs_i MR_i^1_{0 n2}, so
+//   G = noise F + sum_{n2} nu[n2] sum_{l1} w(l1, n2) F^{l1}_{m, n-n2}.
+template <typename T> __host__ __device__ constexpr size_t local_tile_bytes(int rmax, int W) {
+  return ((size_t)rmax * W * sizeof(c2<T>) + 15) / 16 * 16;
+}
+
 template <typename T, int W, int NDIM>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __restrict__ F,
-                                               c2<T>* __restrict__ G, const int* __restrict__ tap_row,
-                                               const int* __restrict__ tap_cnt,
-                                               const double2* __restrict__ tap_w, DerivParams prm) {
+                                               c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
+                                               const c2<T>* __restrict__ Gx, DerivParams prm) {
   using C = c2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* tile = reinterpret_cast<C*>(smraw);     // [rows of the group][W]
   const int D = 2 * L.lmax + 1;
+  const int rmax = (L.lmax + 1) * (L.lmax + 1);
+  C* tile = reinterpret_cast<C*>(smraw);                                          // [R][W]
+  T* sw = reinterpret_cast<T*>(smraw + local_tile_bytes<T>(rmax, W));             // [R][9]
+  int* sseg = reinterpret_cast<int*>(smraw + local_tile_bytes<T>(rmax, W) +
+                                     ((size_t)rmax * 9 * sizeof(T) + 15) / 16 * 16);  // [D]
   const int m = (int)blockIdx.y + L.m_lo;
   const int r0 = L.seg[(m - L.m_lo) * D];
   const int r1 = (m + 1 <= L.lmax) ? L.seg[(m + 1 - L.m_lo) * D] : (int)L.nrows;
   const int R = r1 - r0;
   const long long w0 = (long long)blockIdx.x * W;
   const int tid = threadIdx.x, nth = blockDim.x;
-  // group rows staged with 4 loads in flight per thread
-  for (int e0 = tid; e0 < R * W; e0 += 4 * nth) {
-    C v[4];
+  // group rows staged with 8 loads in flight per thread
+  for (int e0 = tid; e0 < R * W; e0 += 8 * nth) {
+    C v[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * nth;
       const int r = e / W, w = e % W;
       v[u] = (e < R * W && w0 + w < L.nx) ? cvt<C, double2>(F[(size_t)(r0 + r) * L.nx + w0 + w]) : czero<C>();
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * nth;
       if (e < R * W) tile[e] = v[u];
     }
   }
+  for (int e = tid; e < R * 9; e += nth) sw[e] = tap_wr[(size_t)r0 * 9 + e];
+  for (int e = tid; e < D; e += nth) sseg[e] = L.seg[(m - L.m_lo) * D + e] - r0;
   __syncthreads();
   const int w = tid % W, rl = tid / W, nrl = nth / W;
   const long long wg = w0 + w;
@@ -111,40 +123,69 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
       dd[a] = tp * (T)kappa_diag(k, N);
     }
   }
-  T d1g[NDIM];  // D_i times the gravity scale of component i
-#pragma unroll
-  for (int a = 0; a < NDIM; ++a) d1g[a] = d1[a] * (T)prm.gs[a];
   T noise = 0;
 #pragma unroll
   for (int i = 0; i < NDIM; ++i)
 #pragma unroll
     for (int j = 0; j < NDIM; ++j)
       noise -= (T)prm.G[i * 3 + j] * ((i == j) ? dd[i] * dd[i] : d1[i] * d1[j]);
+  C nu[3];  // -i sum_i d1_i gs_i MR_i^1_{0 n2}
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    T mx = 0, my = 0;
+#pragma unroll
+    for (int i = 0; i < NDIM; ++i) {
+      const T s = d1[i] * (T)prm.gs[i];
+      mx += s * (T)prm.mr[q][i][0];
+      my += s * (T)prm.mr[q][i][1];
+    }
+    nu[q].x = my;
+    nu[q].y = -mx;
+  }
+  const int am = abs(m), lmax = L.lmax;
   for (int r = rl; r < R; r += nrl) {
-    const int rg = r0 + r;
+    const char4 q = L.rows[r0 + r];
+    const int l = q.x, n = q.z;
     const C f0 = tile[r * W + w];
     T ax = noise * f0.x, ay = noise * f0.y;
-    const int cnt = tap_cnt[rg];
-    for (int t = 0; t < cnt; ++t) {
-      const int src = tap_row[rg * 9 + t];
-      // coef = -sum_i (i d1_i) W_i = sum_i d1_i (W_i.y - i W_i.x)
-      T cx = 0, cy = 0;
 #pragma unroll
-      for (int i = 0; i < NDIM; ++i) {
-        const double2 wv = tap_w[(rg * 9 + t) * 3 + i];
-        cx += d1g[i] * (T)wv.y;
-        cy -= d1g[i] * (T)wv.x;
+    for (int n2o = 0; n2o < 3; ++n2o) {
+      const int n1 = n - (n2o - 1);
+      if (n1 < -lmax || n1 > lmax) continue;
+      const int an1 = abs(n1), lo = am > an1 ? am : an1;
+      const int base = sseg[n1 + lmax] - lo;
+      T sx = 0, sy = 0;
+#pragma unroll
+      for (int l1o = 0; l1o < 3; ++l1o) {
+        const T wt = sw[r * 9 + l1o * 3 + n2o];
+        if (wt != (T)0) {
+          const C fs = tile[(base + l + l1o - 1) * W + w];
+          sx += wt * fs.x;
+          sy += wt * fs.y;
+        }
       }
-      const C fs = tile[(src - r0) * W + w];
-      ax += cx * fs.x - cy * fs.y;
-      ay += cx * fs.y + cy * fs.x;
+      ax += nu[n2o].x * sx - nu[n2o].y * sy;
+      ay += nu[n2o].x * sy + nu[n2o].y * sx;
+    }
+    if (Gx) {  // density-side gravity term (density-gravity models)
+      const C gx = Gx[(size_t)(r0 + r) * L.nx + wg];
+      ax += gx.x;
+      ay += gx.y;
     }
     C o;
     o.x = ax;
     o.y = ay;
-    G[(size_t)rg * L.nx + wg] = o;
+    G[(size_t)(r0 + r) * L.nx + wg] = o;
   }
 }
+
+template <typename T> static size_t local_smem(const hp_plan* p, int W) {
+  const int rmax = (p->lmax + 1) * (p->lmax + 1);
+  return local_tile_bytes<T>(rmax, W) + ((size_t)rmax * 9 * sizeof(T) + 15) / 16 * 16 + sizeof(int) * p->D;
+}
+template <typename T> static const T* tap_table(const hp_plan* p);
+template <> const double* tap_table<double>(const hp_plan* p) { return p->tap_wr; }
+template <> const float* tap_table<float>(const hp_plan* p) { return p->tap_wr32; }
 
 template <typename T> static constexpr int local_w() { return sizeof(T) == 8 ? 16 : 32; }
 
@@ -170,7 +211,6 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
                                                   const double2* __restrict__ Fev,
                                                   const c2<T>* __restrict__ P3,
                                                   const c2<T>* __restrict__ Gl,
-                                                  const c2<T>* __restrict__ Gx,
                                                   const double2* __restrict__ F0, double a,
                                                   double2* __restrict__ out,
                                                   double2* __restrict__ acc, double bacc,
@@ -396,7 +436,6 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const
           const int c = e / (N * N), q = e % (N * N);
           gi[u] = row_of(L, tl.l, tl.m, tl.n0 + c) * L.nx + pbase + q;
           g[u] = Gl[gi[u]];
-          if (Gx) g[u] = g[u] + Gx[gi[u]];
           f0[u] = F0 ? F0[gi[u]] : make_double2(0.0, 0.0);
           if (acc) ac[u] = acc[gi[u]];
         }
@@ -452,15 +491,15 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   }
   {
     constexpr int W = local_w<T>();
-    const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
+    const size_t lsm = local_smem<T>(p, W);
     dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
     ProfScope _ps(p, "deriv.local", s);
     if (p->ndim == 3) {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 3><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+      k_local<T, W, 3><<<grid, 256, lsm, s>>>(L, Fev, G, tap_table<T>(p), (const C*)Gx, prm);
     } else {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 2><<<grid, 256, lsm, s>>>(L, Fev, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+      k_local<T, W, 2><<<grid, 256, lsm, s>>>(L, Fev, G, tap_table<T>(p), (const C*)Gx, prm);
     }
     HP_CUDA_TRY(cudaGetLastError());
   }
@@ -484,10 +523,10 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   ProfScope _ps(p, "deriv.plane", s);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, (const C*)Gx, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, (const C*)Gx, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -567,6 +606,11 @@ DerivParams hp_model_params(const hp_plan* p) {
   for (int i = 0; i < 3; ++i) { prm.b[i] = p->model.b[i]; prm.gyro[i] = p->model.gyro[i]; prm.gs[i] = 1.0; }
   for (int i = 0; i < 9; ++i) prm.G[i] = p->model.G[i];
   prm.lie = 1.0;
+  for (int q = 0; q < 3; ++q)
+    for (int i = 0; i < 3; ++i) {
+      prm.mr[q][i][0] = p->mr1[q][i].x;
+      prm.mr[q][i][1] = p->mr1[q][i].y;
+    }
   if (p->ndim == 2) { prm.b[2] = 0; prm.gyro[0] = prm.gyro[1] = prm.gyro[2] = 0; }
   return prm;
 }
@@ -669,14 +713,14 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   }
   {
     constexpr int W = local_w<T>();
-    const size_t lsm = sizeof(C) * (size_t)(p->lmax + 1) * (p->lmax + 1) * W;
+    const size_t lsm = local_smem<T>(p, W);
     const dim3 lg((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
     if (p->ndim == 3) {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 3><<<lg, 256, lsm, s>>>(L, Fi, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+      k_local<T, W, 3><<<lg, 256, lsm, s>>>(L, Fi, G, tap_table<T>(p), nullptr, prm);
     } else {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 2><<<lg, 256, lsm, s>>>(L, Fi, G, p->tap_row, p->tap_cnt, p->tap_w, prm);
+      k_local<T, W, 2><<<lg, 256, lsm, s>>>(L, Fi, G, tap_table<T>(p), nullptr, prm);
     }
   }
   HP_CUDA_TRY(cudaGetLastError());
@@ -684,10 +728,10 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   dim3 grid((unsigned)ntiles, p3 ? N : 1);
   if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return hp_internal_to_full(p, dFi, dFfull, s);

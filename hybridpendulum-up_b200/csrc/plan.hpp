@@ -56,9 +56,9 @@ struct hp_plan {
   // model
   bool has_model = false;
   hp_model model{};
-  int* tap_row = nullptr;    // [row][9] source rows of the non-zero taps
-  int* tap_cnt = nullptr;    // [row] number of non-zero taps
-  double2* tap_w = nullptr;  // [row][9][3] weights per component
+  double* tap_wr = nullptr;  // [row][9] real gravity tap weights, tap (l1-l+1)*3 + (n2+1)
+  float* tap_wr32 = nullptr;
+  double2 mr1[3][3] = {};    // MR_i^1_{0 n2} of the model: [n2+1][i]
   double* den_mR = nullptr;  // [2][(2B)^3] density-side gravity multipliers (pendulum_reduced_den)
 
   // profiling
@@ -116,7 +116,7 @@ struct ProfScope {
 // ---- launchers implemented in the .cu files (return hp_status) ----
 int hp_tables_build(hp_plan* p);
 int hp_twiddles_init();
-int hp_build_gravity_taps(hp_plan* p, const double2* MR_full_dev);
+int hp_build_gravity_taps(hp_plan* p);
 int hp_full_to_internal(hp_plan* p, const double2* Ffull, double2* Fint, cudaStream_t s);
 int hp_internal_to_full(hp_plan* p, const double2* Fint, double2* Ffull, cudaStream_t s);
 // Coefficients of the derivative terms: lie scales the Lie (u) term, gs[i]
@@ -129,6 +129,7 @@ struct DerivParams {
   double gyro[3];
   double lie;
   double gs[3];
+  double mr[3][3][2];  // MR_i^1_{0 n2}: [n2+1][i][re, im]
 };
 DerivParams hp_model_params(const hp_plan* p);
 int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Feval, const double2* F0,

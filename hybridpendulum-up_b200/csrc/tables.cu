@@ -113,40 +113,27 @@ __global__ void k_cg1(int lmax, double* cg1) {
 
 // Gravity taps: Grav_i^l_{mn} = sum_{l1, n2} W F^{l1}_{m, n-n2}, with
 // W = (2l1+1)*3/(2l+1) <l1 m; 1 0|l m><l1 n-n2; 1 n2|l n> MR_i^1_{0 n2}
-// (the l2 = 1, m2 = 0 terms of the CG loop of pendulum.m:474-502).  Stored
-// compactly per row: tap_row[row*9 + 0..cnt) the source rows, tap_row[row*9+8]
-// holds cnt when cnt < 9 is needed, and tap_w[(row*9 + t)*3 + i] the weights.
-__global__ void k_gravity_taps(RowLayout L, const double* __restrict__ cg1,
-                               const double2* __restrict__ MR, int* __restrict__ tap_row,
-                               int* __restrict__ tap_cnt, double2* __restrict__ tap_w) {
+// (the l2 = 1, m2 = 0 terms of the CG loop of pendulum.m:474-502).  The
+// weight factors into a real part per tap, stored here as
+// tap_wr[row*9 + (l1-l+1)*3 + (n2+1)] (zero where the source row does not
+// exist), and the model's MR_i^1_{0 n2}, applied per omega point.
+template <typename T>
+__global__ void k_gravity_taps(RowLayout L, const double* __restrict__ cg1, T* __restrict__ tap_wr) {
   const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (r >= L.nrows) return;
-  const int lmax = L.lmax, D = 2 * lmax + 1;
+  const int lmax = L.lmax;
   const char4 q = L.rows[r];
   const int l = q.x, m = q.y, n = q.z;
-  int cnt = 0;
   for (int t = 0; t < 9; ++t) {
     const int l1 = l + t / 3 - 1, n2 = t % 3 - 1, n1 = n - n2;
-    if (!(l1 >= 0 && l1 <= lmax && abs(m) <= l1 && abs(n1) <= l1 && abs(l - l1) <= 1)) continue;
-    const double cm = cg1[cg1_index(lmax, l1, l - l1, m, 0)];
-    const double cn = cg1[cg1_index(lmax, l1, l - l1, n, n2)];
-    const double w = (2.0 * l1 + 1.0) * 3.0 / (2.0 * l + 1.0) * cm * cn;
-    double2 wi[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-    bool any = false;
-    for (int i = 0; i < L.ndim; ++i) {
-      // MR(m2+lmax+1, n2+lmax+1, 2, i) with m2 = 0, l2 = 1
-      const double2 mr = MR[(lmax) + (long long)D * (n2 + lmax) + (long long)D * D * 1 +
-                            (long long)D * D * (lmax + 1) * i];
-      wi[i] = make_double2(w * mr.x, w * mr.y);
-      any = any || wi[i].x != 0.0 || wi[i].y != 0.0;
+    double w = 0.0;
+    if (l1 >= 0 && l1 <= lmax && abs(m) <= l1 && abs(n1) <= l1) {
+      const double cm = cg1[cg1_index(lmax, l1, l - l1, m, 0)];
+      const double cn = cg1[cg1_index(lmax, l1, l - l1, n, n2)];
+      w = (2.0 * l1 + 1.0) * 3.0 / (2.0 * l + 1.0) * cm * cn;
     }
-    if (!any) continue;
-    const int am = abs(m), an = abs(n1);
-    tap_row[r * 9 + cnt] = L.seg[(m - L.m_lo) * D + n1 + lmax] + l1 - (am > an ? am : an);
-    for (int i = 0; i < 3; ++i) tap_w[(r * 9 + cnt) * 3 + i] = wi[i];
-    ++cnt;
+    tap_wr[r * 9 + t] = (T)w;
   }
-  tap_cnt[r] = cnt;
 }
 
 // ------------------------------------------------ layout conversions ----
@@ -287,14 +274,13 @@ int hp_tables_build(hp_plan* p) {
   return HP_OK;
 }
 
-int hp_build_gravity_taps(hp_plan* p, const double2* MR_dev) {
-  if (!p->tap_row) {
-    HP_CUDA_TRY(cudaMalloc(&p->tap_row, sizeof(int) * 9 * p->nrows));
-    HP_CUDA_TRY(cudaMalloc(&p->tap_cnt, sizeof(int) * p->nrows));
-    HP_CUDA_TRY(cudaMalloc(&p->tap_w, sizeof(double2) * 9 * 3 * p->nrows));
-  }
-  k_gravity_taps<<<(unsigned)((p->nrows + 127) / 128), 128, 0, p->stream>>>(p->layout(), p->cg1, MR_dev,
-                                                                           p->tap_row, p->tap_cnt, p->tap_w);
+int hp_build_gravity_taps(hp_plan* p) {
+  if (p->tap_wr) return HP_OK;
+  HP_CUDA_TRY(cudaMalloc(&p->tap_wr, sizeof(double) * 9 * p->nrows));
+  HP_CUDA_TRY(cudaMalloc(&p->tap_wr32, sizeof(float) * 9 * p->nrows));
+  const unsigned g = (unsigned)((p->nrows + 127) / 128);
+  k_gravity_taps<double><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr);
+  k_gravity_taps<float><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr32);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }

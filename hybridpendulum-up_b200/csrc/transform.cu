@@ -12,6 +12,7 @@
 //      the Hermitian reconstruction of ifftn(..., 'symmetric').
 // Forward (fftSO3R.m:89-106) runs the same stages in reverse with the
 // quadrature weights w_b.
+#include <algorithm>
 #include <vector>
 #include "common.cuh"
 #include "plan.hpp"
@@ -108,6 +109,14 @@ __global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out
   if (i < n) out[i] = cvt<double2, c2<T>>(in[i]);
 }
 
+// 16-byte global store of values read one by one from shared memory
+__device__ __forceinline__ void store16(float* dst, const float* s) {
+  *reinterpret_cast<float4*>(dst) = make_float4(s[0], s[1], s[2], s[3]);
+}
+__device__ __forceinline__ void store16(double* dst, const double* s) {
+  *reinterpret_cast<double2*>(dst) = make_double2(s[0], s[1]);
+}
+
 // ------------------------------------------------------------ synthesis ----
 // Block = (group of NB consecutive beta indices, range of omega points), the
 // (2l+1)-weighted d values of its betas resident in shared memory.  Input rows
@@ -116,8 +125,8 @@ __global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out
 // beta) intermediates G -> H live in shared memory as [bb][m][q][p].
 template <int B, typename T, int NB, int P, bool CPLX>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
-                                                  const T* __restrict__ wig, void* __restrict__ fout,
-                                                  int nbatch) {
+                                                  const T* __restrict__ wig, const int2* __restrict__ pairs,
+                                                  void* __restrict__ fout, int nbatch) {
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
   constexpr int NM = CPLX ? D : B;
@@ -126,7 +135,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nrows = (int)L.nrows;
   T* sd = reinterpret_cast<T*>(smraw);
-  C* sG = reinterpret_cast<C*>(smraw + ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16);
+  int2* spairs = reinterpret_cast<int2*>(smraw + ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16);
+  C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
   // beta groups of one omega chunk are consecutive blocks, so they read the
   // same coefficient rows close together in time (L2 reuse)
   constexpr int NGROUPS = (NB2 + NB - 1) / NB;
@@ -140,37 +150,43 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
     const T l2 = (T)(2 * L.rows[r].x + 1);
     sd[e] = (bb < nbv) ? l2 * wig[(size_t)(b0 + bb) * nrows + r] : (T)0;
   }
+  for (int e = tid; e < NPAIR; e += nth) spairs[e] = pairs[e];
   const long long nx = L.nx;
   for (int bt = 0; bt < nbatch; ++bt) {
     const long long w0 = ((long long)chunk * nbatch + bt) * P;
     if (w0 >= nx) break;
     __syncthreads();
-    // beta stage: item (pair, p), p fastest
+    // beta stage: item (pair, p), p fastest.  Pairs come from the block's copy
+    // of the pair table (longest l-runs first, so the lanes of a warp run
+    // loops of similar length); the l-run is loaded in batches of 8 ahead of
+    // its FMAs, each coefficient feeding NB FMAs per component.
     for (int it = tid; it < NPAIR * P; it += nth) {
-      const int p = it % P, pr = it / P;
-      const int mi = pr / D, n = pr % D - lmax, m = mi + MLO;
-      const int am = abs(m), an = abs(n), lmin = am > an ? am : an;
-      const int q = n >= 0 ? n : n + NB2;
+      const int p = it % P;
+      const int2 pe = spairs[it / P];
+      const int s = pe.x, len = pe.y & 0xff, mi = (pe.y >> 8) & 0xff, q = (pe.y >> 16) & 0xff;
       C acc[NB];
 #pragma unroll
       for (int bb = 0; bb < NB; ++bb) acc[bb] = czero<C>();
       if (w0 + p < nx) {
-        const int s = L.seg[(m - L.m_lo) * D + n + lmax];
         const C* src = Fp + (size_t)s * nx + w0 + p;
         const T* dsrc = sd + (size_t)s * NB;
-        const int len = lmax - lmin + 1;
-        // loads issued in batches of 4 ahead of their FMAs
-        for (int j0 = 0; j0 < len; j0 += 4) {
-          C v[4];
+        constexpr int JB = 8;
 #pragma unroll
-          for (int u = 0; u < 4; ++u) v[u] = (j0 + u < len) ? src[(size_t)(j0 + u) * nx] : czero<C>();
+        for (int j0 = 0; j0 < B; j0 += JB) {
+          if (j0 < len) {
+            C v[JB];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < JB; ++u) v[u] = (j0 + u < len) ? src[(size_t)(j0 + u) * nx] : czero<C>();
 #pragma unroll
-            for (int bb = 0; bb < NB; ++bb) {
-              const T dv = (j0 + u < len) ? dsrc[(j0 + u) * NB + bb] : (T)0;
-              acc[bb].x = fma(dv, v[u].x, acc[bb].x);
-              acc[bb].y = fma(dv, v[u].y, acc[bb].y);
+            for (int u = 0; u < JB; ++u) {
+              if (j0 + u < len) {
+#pragma unroll
+                for (int bb = 0; bb < NB; ++bb) {
+                  const T dv = dsrc[(j0 + u) * NB + bb];
+                  acc[bb].x = fma(dv, v[u].x, acc[bb].x);
+                  acc[bb].y = fma(dv, v[u].y, acc[bb].y);
+                }
+              }
             }
           }
         }
@@ -179,7 +195,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
       for (int bb = 0; bb < NB; ++bb) {
         C* g = sG + ((bb * NM + mi) * NB2) * P + p;
         g[q * P] = acc[bb];
-        if (n == 0) g[B * P] = czero<C>();
+        if (pe.y >> 24) g[B * P] = czero<C>();
       }
     }
     __syncthreads();
@@ -238,8 +254,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
       } else {
-        T* st = reinterpret_cast<T*>(sG) + ((p * NB2 + c) * NB + bb) * NB2;
-        T* st2 = reinterpret_cast<T*>(sG) + ((p * NB2 + c + B) * NB + bb) * NB2;
+        // runs of NB*2B values per (p, c) padded by one element: consecutive
+        // threads of a warp then write distinct banks
+        constexpr int RS = NB * NB2 + 1;
+        T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS + bb * NB2;
+        T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS + bb * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) {
           st[a] = x[a].x;
@@ -249,27 +268,26 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
     }
     __syncthreads();
     // store: f[a + 2B (b + 2B (c + 2B w))]; the nbv*2B values of one (w, c) are
-    // contiguous in f and in the staging buffer, one thread copies one run.
+    // contiguous in f and in the staging buffer; a warp copies one run with
+    // consecutive lanes on consecutive 16-byte pieces.
     const int pc = (int)min((long long)P, nx - w0);
     constexpr int RUN = NB * NB2;
-    for (int e = tid; e < pc * NB2; e += nth) {
-      const int pp = e / NB2, cc = e % NB2;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    for (int run = warp; run < pc * NB2; run += nwarps) {
+      const int pp = run / NB2, cc = run % NB2;
       const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2;
-      const int si = (pp * NB2 + cc) * RUN;
       if (CPLX) {
         C* dst = reinterpret_cast<C*>(fout) + gi;
-        for (int o = 0; o < nbv * NB2; ++o) dst[o] = sG[si + o];
+        const C* src = sG + (pp * NB2 + cc) * RUN;
+        for (int o = lane; o < nbv * NB2; o += 32) dst[o] = src[o];
       } else {
         T* dst = reinterpret_cast<T*>(fout) + gi;
-        const T* src = reinterpret_cast<const T*>(sG) + si;
+        const T* src = reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * (RUN + 1);
         constexpr int VW = 16 / sizeof(T);   // elements per 16-byte vector
-        const bool vec = nbv == NB && (RUN % VW) == 0 && ((gi % VW) == 0) && ((si % VW) == 0);
-        if (vec) {
-#pragma unroll
-          for (int o = 0; o < RUN; o += VW)
-            *reinterpret_cast<float4*>(dst + o) = *reinterpret_cast<const float4*>(src + o);
+        if (nbv == NB && (RUN % VW) == 0 && (gi % VW) == 0) {
+          for (int o = lane * VW; o < RUN; o += 32 * VW) store16(dst + o, src + o);
         } else {
-          for (int o = 0; o < nbv * NB2; ++o) dst[o] = src[o];
+          for (int o = lane; o < nbv * NB2; o += 32) dst[o] = src[o];
         }
       }
     }
@@ -444,15 +462,22 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr int NCOL = CPLX ? 2 * B : B;
   static constexpr long long bytes(int nb, int p) {
     const long long g = (long long)NM * 2 * B * 2 * (long long)sizeof(T);            // G/H, complex
-    const long long st = (long long)2 * B * 2 * B * (CPLX ? 2 : 1) * (long long)sizeof(T);  // f staging
-    return nb * nrows * (long long)sizeof(T) + 16 + (long long)nb * p * (g > st ? g : st);
+    const long long st = CPLX ? (long long)2 * B * 2 * B * 2 * (long long)sizeof(T)  // f staging
+                              : (long long)2 * B * (2 * B + 1) * (long long)sizeof(T);  // (runs padded by 1 per nb)
+    return nb * nrows * (long long)sizeof(T) + 32 + (long long)NM * (2 * B - 1) * 8 +
+           (long long)nb * p * (g > st ? g : st);
   }
   // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB)
   static constexpr long long budget() { return bytes(1, 4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
-  static constexpr int pick_nb() { return bytes(2, 4) <= budget() ? 2 : 1; }
+  // betas per block: up to 4 (each coefficient then feeds 4 x P FMAs), as
+  // many as keep a batch of 4 omega points within the budget
+  static constexpr int pick_nb() {
+    return bytes(4, 4) <= budget() && 4 * NCOL * 4 <= 256 ? 4
+         : bytes(2, 4) <= budget() ? 2 : 1;
+  }
   static constexpr int NB = pick_nb();
   static constexpr int pick_p() {
-    int p = 8;
+    int p = NB >= 4 ? 4 : 8;
     while (p > 1 && (bytes(NB, p) > budget() || NB * NCOL * p > 256)) p /= 2;
     return p;
   }
@@ -467,11 +492,43 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   static_assert(NB * Cfg::NCOL * P <= 256, "alpha stage must fit one round");
   const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
   const size_t sg_bytes = std::max((size_t)NB * NM * NB2 * P * sizeof(C),
-                                   (size_t)P * NB2 * NB * NB2 * (CPLX ? sizeof(C) : sizeof(T)));
-  const size_t smem = sd_bytes + sg_bytes;
+                                   CPLX ? (size_t)P * NB2 * NB * NB2 * sizeof(C)
+                                        : (size_t)P * NB2 * (NB * NB2 + 1) * sizeof(T));
+  constexpr int NPAIR = NM * (2 * B - 1);
+  const size_t pr_bytes = ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16;
+  const size_t smem = sd_bytes + pr_bytes + sg_bytes;
   if (smem > (size_t)smem_limit()) {
     hp_set_error("synthesis tables exceed shared memory for this bandlimit");
     return HP_ERR_UNSUPPORTED;
+  }
+  int st = HP_OK;
+  const char* key = CPLX ? "tf.pairs_c" : "tf.pairs_r";
+  bool have = false;
+  for (auto& kv : p->ws) if (kv.first == key) have = true;
+  int2* dpairs = (int2*)p->ws_get(key, sizeof(int2) * NPAIR, &st);
+  if (st) return st;
+  if (!have) {
+    // (m, n) pairs with their row start, l-run length, m slot and n bin,
+    // longest runs first
+    std::vector<std::pair<int, int2>> v;
+    const int lmax = B - 1, D = 2 * lmax + 1, mlo = CPLX ? -lmax : 0;
+    for (int mi = 0; mi < NM; ++mi)
+      for (int n = -lmax; n <= lmax; ++n) {
+        const int m = mi + mlo;
+        const int lmin = std::max(std::abs(m), std::abs(n));
+        const int len = lmax - lmin + 1;
+        const int q = n >= 0 ? n : n + NB2;
+        int2 e;
+        e.x = p->h_seg[(size_t)(m - p->m_lo) * D + n + lmax];
+        e.y = len | (mi << 8) | (q << 16) | ((n == 0 ? 1 : 0) << 24);
+        v.push_back({len, e});
+      }
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int2>& a, const std::pair<int, int2>& b) {
+      return a.first > b.first;
+    });
+    std::vector<int2> h;
+    for (auto& x : v) h.push_back(x.second);
+    HP_CUDA_TRY(cudaMemcpy(dpairs, h.data(), sizeof(int2) * NPAIR, cudaMemcpyHostToDevice));
   }
   const int ngroups = (NB2 + NB - 1) / NB;
   const long long nbatches = (p->nx + P - 1) / P;
@@ -485,7 +542,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   k_synth<B, T, NB, P, CPLX><<<grid, 256, smem, s>>>(p->layout(), Fp,
                                                      p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
                                                                              : (const T*)(const void*)p->wig32,
-                                                     f, nbatch);
+                                                     dpairs, f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
