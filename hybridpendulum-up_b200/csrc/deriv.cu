@@ -193,8 +193,8 @@ template <typename T> static constexpr int local_w() { return sizeof(T) == 8 ? 1
 struct PlaneTile { int m, l, n0, cnt; };
 
 template <typename T> struct PlaneCfg;
-template <> struct PlaneCfg<double> { static constexpr int C = 1; static constexpr int NT = 128; };
-template <> struct PlaneCfg<float> { static constexpr int C = 2; static constexpr int NT = 256; };
+template <> struct PlaneCfg<double> { static constexpr int C = 1; static constexpr int NT = 128; static constexpr int MINB = 2; };
+template <> struct PlaneCfg<float> { static constexpr int C = 2; static constexpr int NT = 256; static constexpr int MINB = 2; };
 
 __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, int n) {
   const int am = abs(m), an = abs(n);
@@ -207,7 +207,7 @@ __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, in
 //   [2C+2, 3C+2)       A  = FFT2(Y0) + D_2 FFT2(Y2), then FFT_1
 //   [3C+2, 4C+2)       Y1' = FFT_2(Y1), then D_1 FFT_1
 template <int N, typename T, bool HAS_P3>
-__global__ void __launch_bounds__(PlaneCfg<T>::NT, 2) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
                                                   const double2* __restrict__ Fev,
                                                   const c2<T>* __restrict__ P3,
                                                   const c2<T>* __restrict__ Gl,
@@ -505,7 +505,7 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   }
   // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
   constexpr int CT = PlaneCfg<T>::C;
-  const char* tkey = CT == 2 ? "deriv.tiles2" : "deriv.tiles4";
+  const char tkey[] = {'d', 'e', 'r', 'i', 'v', '.', 't', 'i', 'l', 'e', 's', (char)('0' + CT), 0};
   bool have = false;
   for (auto& kv : p->ws) if (kv.first == tkey) have = true;
   std::vector<PlaneTile> htiles;
