@@ -42,7 +42,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_derivative_noalloc', 'hp_state_normalize', 'hp_collision_create',
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
-           'hp_pendulum_adjoint']
+           'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments']
 
 
 class HPError(RuntimeError):
@@ -59,6 +59,20 @@ class hp_model(ctypes.Structure):
 class hp_model_grad(ctypes.Structure):
     _fields_ = [('b', ctypes.c_double * 3), ('G', ctypes.c_double * 9), ('gyro', ctypes.c_double * 3),
                 ('gscale', ctypes.c_double * 3)]
+
+
+class hp_moments_t(ctypes.Structure):
+    _fields_ = [('mass', ctypes.c_double), ('ER', ctypes.c_double * 9), ('ERR', ctypes.c_double * 81),
+                ('Ex', ctypes.c_double * 3), ('Exx', ctypes.c_double * 9), ('ExR', ctypes.c_double * 27)]
+
+
+def _moments_dict(m: 'hp_moments_t', nd: int, fx) -> dict:
+    out = dict(mass=m.mass, ER=np.array(m.ER[:]).reshape(3, 3), ERR=np.array(m.ERR[:]).reshape(3, 3, 3, 3),
+               Ex=np.array(m.Ex[:nd]), Exx=np.array(m.Exx[:]).reshape(3, 3)[:nd, :nd],
+               ExR=np.array(m.ExR[:]).reshape(3, 3, 3)[:nd])
+    if fx is not None:
+        out['fx'] = fx
+    return out
 
 
 class hp_collision_params(ctypes.Structure):
@@ -103,6 +117,8 @@ def _load():
         'hp_pendulum_propagate_den': [vp, vp, vp, vp, dp, ip, ip],
         'hp_state_hybrid_step': [vp, vp, dp, ip, ip],
         'hp_pendulum_derivative_adjoint': [vp, vp, vp, ip],
+        'hp_moments': [vp, vp, ip, ctypes.POINTER(hp_moments_t), vp],
+        'hp_state_moments': [vp, ctypes.POINTER(hp_moments_t), vp],
         'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
     }
     for name, args in sig.items():
@@ -309,6 +325,17 @@ class Plan:
                                               ctypes.c_void_p(po), float(dt), METHODS[method.lower()], mi))
         return out
 
+    def moments(self, F, want_fx: bool = False) -> dict:
+        """Raw moments of get_stat (mass, ER, ERR, Ex, Exx, ExR; fx on request)
+        of the density with coefficients F, from the coefficients alone."""
+        F = _as_matlab(F, np.complex128)
+        pf, mf = _ptr(F, np.complex128)
+        m = hp_moments_t()
+        fx = np.zeros((self.N,) * self.ndim, order='F') if want_fx else None
+        _check(_lib.hp_moments(self._h, ctypes.c_void_p(pf), mf, ctypes.byref(m),
+                               ctypes.c_void_p(fx.ctypes.data if want_fx else None)))
+        return _moments_dict(m, self.ndim, fx)
+
     def derivative_adjoint(self, lam, out=None):
         """A^H lam, the adjoint of ``derivative`` under <X, Y> = Re sum conj(X) Y."""
         lam = _as_matlab(lam, np.complex128)
@@ -396,6 +423,15 @@ class State:
         if coll.plan is not self.plan:
             raise ValueError('the collision operator must be built on the state plan')
         _check(_lib.hp_state_hybrid_step(self._h, coll._h, float(dt), METHODS[method.lower()], int(nsteps)))
+
+    def moments(self, want_fx: bool = False) -> dict:
+        """Raw moments of get_stat of the resident density (after hybrid steps:
+        of the post-collision grid density)."""
+        m = hp_moments_t()
+        fx = np.zeros((self.plan.N,) * self.plan.ndim, order='F') if want_fx else None
+        _check(_lib.hp_state_moments(self._h, ctypes.byref(m),
+                                     ctypes.c_void_p(fx.ctypes.data if want_fx else None)))
+        return _moments_dict(m, self.plan.ndim, fx)
 
     def density_into(self, dev_ptr: int):
         _check(_lib.hp_state_density(self._h, ctypes.c_void_p(dev_ptr)))

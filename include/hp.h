@@ -225,6 +225,25 @@ int hp_collision_tables(hp_collision* coll, double* lambda, int* indR, double* o
                         short* fcL_indx, double* PC, int mem);
 int hp_collision_df(hp_collision* coll, const double* f, double* df, int mem);
 
+/* ---- statistics: the raw moments of get_stat (propagation/pendulum.m:547-594,
+ * pendulum_reduced_hybrid.m:304-351) ----
+ * The moments are computed from the coefficients (F^l_mn with l <= 2 at the
+ * omega origin and l <= 1 along the omega axes), which equal the reference's
+ * grid sums over f; no pass over the grid density is made.  E[.] denotes
+ * c0 sum_grid w_beta (.) f with c0 = (L/2Bx)^n (unnormalised, like get_stat). */
+typedef struct {
+  double mass;       /* E[1]                                               */
+  double ER[9];      /* E[R_kq], index k*3+q                               */
+  double ERR[81];    /* E[R_kq R_k'q'], index (k*3+q)*9 + k'*3+q'          */
+  double Ex[3];      /* E[x_i] (i < ndim)                                  */
+  double Exx[9];     /* E[x_i x_j], index i*3+j (raw, not centred)         */
+  double ExR[27];    /* E[x_i R_kq], index i*9 + k*3+q                     */
+} hp_moments_t;
+/* Moments of the density with coefficients F (full layout).  fx (may be NULL):
+ * host buffer of (2Bx)^ndim doubles receiving the R-marginal sum_R w f on the
+ * omega grid (first omega index fastest).  Needs B >= 3 and a model (for L). */
+int hp_moments(hp_plan* plan, const double* F, int mem, hp_moments_t* out, double* fx);
+
 /* ---- resident state: coefficients kept on the device in the plan's internal
  * layout across steps (the time loops of pendulum.m:269-315 and
  * pendulum_reduced.m:243-289 without host round trips). ---- */
@@ -247,6 +266,9 @@ int hp_state_hybrid_step(hp_state* state, hp_collision* coll, double dt, int met
 int hp_state_density(hp_state* state, void* f);
 /* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
 int hp_state_mass(hp_state* state, double* mass);
+/* hp_moments of the resident state; after hybrid steps these are the moments
+ * of the post-collision grid density (its forward transform is the state). */
+int hp_state_moments(hp_state* state, hp_moments_t* out, double* fx);
 /* l = 0 mass normalisation: scales the state (FP64) so that F^0_{00}[0] == mass;
  * *scale (may be NULL) receives the factor applied.  The derivative conserves
  * F^0_{00}[0] exactly (every term vanishes at l = 0, k = 0), so this only
