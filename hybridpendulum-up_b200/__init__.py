@@ -42,7 +42,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_derivative_noalloc', 'hp_state_normalize', 'hp_collision_create',
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
-           'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments']
+           'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
+           'hp_state_init_mf_gauss']
 
 
 class HPError(RuntimeError):
@@ -73,6 +74,18 @@ def _moments_dict(m: 'hp_moments_t', nd: int, fx) -> dict:
     if fx is not None:
         out['fx'] = fx
     return out
+
+
+def _mfg_args(U, s, V, mu, Sigma, ndim):
+    U = np.ascontiguousarray(U, float).reshape(3, 3)
+    V = np.ascontiguousarray(V, float).reshape(3, 3)
+    s = np.ascontiguousarray(s, float).reshape(3)
+    mu = np.ascontiguousarray(np.asarray(mu, float).reshape(-1)[:ndim])
+    Sg = np.zeros((3, 3))
+    Sa = np.asarray(Sigma, float)
+    Sg[:Sa.shape[0], :Sa.shape[1]] = Sa
+    arrs = (U, s, V, mu, np.ascontiguousarray(Sg))
+    return arrs, [ctypes.c_void_p(a.ctypes.data) for a in arrs]
 
 
 class hp_collision_params(ctypes.Structure):
@@ -119,6 +132,8 @@ def _load():
         'hp_pendulum_derivative_adjoint': [vp, vp, vp, ip],
         'hp_moments': [vp, vp, ip, ctypes.POINTER(hp_moments_t), vp],
         'hp_state_moments': [vp, ctypes.POINTER(hp_moments_t), vp],
+        'hp_density_mf_gauss': [vp, vp, vp, vp, vp, vp, vp, ip],
+        'hp_state_init_mf_gauss': [vp, vp, vp, vp, vp, vp],
         'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
     }
     for name, args in sig.items():
@@ -325,6 +340,13 @@ class Plan:
                                               ctypes.c_void_p(po), float(dt), METHODS[method.lower()], mi))
         return out
 
+    def density_mf_gauss(self, U, s, V, mu, Sigma):
+        """Matrix Fisher(U diag(s) V^T) x N(mu, Sigma) on the grid (pendulum.m:210-220), FP64."""
+        keep, ptrs = _mfg_args(U, s, V, mu, Sigma, self.ndim)
+        f = np.zeros(self.f_shape, order='F')
+        _check(_lib.hp_density_mf_gauss(self._h, *ptrs, ctypes.c_void_p(f.ctypes.data), HP_HOST))
+        return f
+
     def moments(self, F, want_fx: bool = False) -> dict:
         """Raw moments of get_stat (mass, ER, ERR, Ex, Exx, ExR; fx on request)
         of the density with coefficients F, from the coefficients alone."""
@@ -423,6 +445,11 @@ class State:
         if coll.plan is not self.plan:
             raise ValueError('the collision operator must be built on the state plan')
         _check(_lib.hp_state_hybrid_step(self._h, coll._h, float(dt), METHODS[method.lower()], int(nsteps)))
+
+    def init_mf_gauss(self, U, s, V, mu, Sigma):
+        """Load F = fftSO3R of the matrix Fisher x Gaussian density, built on the device."""
+        keep, ptrs = _mfg_args(U, s, V, mu, Sigma, self.plan.ndim)
+        _check(_lib.hp_state_init_mf_gauss(self._h, *ptrs))
 
     def moments(self, want_fx: bool = False) -> dict:
         """Raw moments of get_stat of the resident density (after hybrid steps:

@@ -143,5 +143,6 @@ int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, doub
 int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* out, cudaStream_t s);
 int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s);
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s);
+int hp_forward_internal64(hp_plan* p, const double* f, double2* Fint, cudaStream_t s);
 int hp_prod_launch(hp_plan* p, const double2* F, const double2* G, double2* FG, int batch,
                    cudaStream_t s);

@@ -540,7 +540,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   dim3 grid((unsigned)(gx * ngroups), 1);
   ProfScope _ps(p, "tf.synth", s);
   k_synth<B, T, NB, P, CPLX><<<grid, 256, smem, s>>>(p->layout(), Fp,
-                                                     p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
+                                                     sizeof(T) == 8 ? (const T*)(const void*)p->wig64
                                                                              : (const T*)(const void*)p->wig32,
                                                      dpairs, f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
@@ -573,7 +573,7 @@ static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa,
   HP_CUDA_TRY(cudaMemsetAsync(Fa, 0, sizeof(C) * p->nrows * p->nx, s));
   ProfScope _ps(p, "tf.anal", s);
   k_anal<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), f,
-                                                      p->precision == HP_FP64 ? (const T*)(const void*)p->wig64
+                                                      sizeof(T) == 8 ? (const T*)(const void*)p->wig64
                                                                               : (const T*)(const void*)p->wig32,
                                                       p->qw, mult, Fa, P, wpb);
   HP_CUDA_TRY(cudaGetLastError());
@@ -672,4 +672,10 @@ int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* o
   const int cplx = p->symmetry == HP_COMPLEX;
   if (p->precision == HP_FP64) return forward_rows_T<double>(p, f, cplx, mult, (double2*)out, s);
   return forward_rows_T<float>(p, f, cplx, mult, (float2*)out, s);
+}
+
+// Forward transform in FP64 whatever the plan's precision (initial densities).
+int hp_forward_internal64(hp_plan* p, const double* f, double2* Fint, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  return forward_T<double>(p, f, 0, Fint, s);   // real density, HP_REAL plans
 }

@@ -225,6 +225,21 @@ int hp_collision_tables(hp_collision* coll, double* lambda, int* indR, double* o
                         short* fcL_indx, double* PC, int mem);
 int hp_collision_df(hp_collision* coll, const double* f, double* df, int mem);
 
+/* ---- initial densities ----
+ * Matrix Fisher x Gaussian on the plan's grid, the initial condition of
+ * propagation/pendulum.m:210-220 (and pendulum_reduced*.m):
+ *   f(R, x) = exp(tr(F^T R)) / c(s) * N(x; mu, Sigma),  F = U diag(s) V^T,
+ * c(s) the matrix Fisher normalising constant ('matrix Fisher/pdf_MF_normal.m').
+ * U, V: 3x3 row-major; s: 3; mu: ndim; Sigma: row-major 3x3 whose leading
+ * ndim x ndim block is used.  The plan's model supplies L.
+ * hp_density_mf_gauss writes f (FP64, grid layout f(a,b,c,x...));
+ * hp_state_init_mf_gauss loads F = fftSO3R(f) (FP64 transform) into the state
+ * without the density leaving the device (HP_REAL plans). */
+int hp_density_mf_gauss(hp_plan* plan, const double* U, const double* s, const double* V, const double* mu,
+                        const double* Sigma, double* f, int mem);
+int hp_state_init_mf_gauss(hp_state* state, const double* U, const double* s, const double* V,
+                           const double* mu, const double* Sigma);
+
 /* ---- statistics: the raw moments of get_stat (propagation/pendulum.m:547-594,
  * pendulum_reduced_hybrid.m:304-351) ----
  * The moments are computed from the coefficients (F^l_mn with l <= 2 at the
