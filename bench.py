@@ -48,6 +48,9 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--fp64-steps', type=int, default=None)
+    ap.add_argument('--workload', default='step', choices=['step', 'batch'],
+                    help='step: the headline FP step; batch: uneven-bandlimit batch of densities')
+    ap.add_argument('--members', type=int, default=64)
     return ap.parse_args()
 
 
@@ -267,6 +270,8 @@ def main():
     local = int(os.environ.get('LOCAL_RANK', '0'))
     B, Bx = args.B, args.Bx
 
+    if args.workload == 'batch':
+        return bench_batch(args, rank, world, local)
     if args.impl == 'reference':
         if rank != 0:
             return 0
@@ -458,6 +463,113 @@ def main():
         'clocks': clocks,
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_batch(args, rank, world, local):
+    """Independent seeded densities with bandlimits B in {8, 12, 16, 20} and
+    omega grids {16^3, 24^3, 32^3} mixed by the seed, advanced together in
+    mixed precision (one CUDA graph per two batch steps, members on distinct
+    plans concurrent), against the per-density FP64 loop.  The step is the
+    plain pendulum propagation (the collision reset map of the reference is
+    defined for 2-D omega only).  Prints one JSON line (not the headline)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    hp = importlib.import_module('hybridpendulum-up_b200')
+    rng = np.random.default_rng(1000 + rank)
+    Bs, Bxs = [8, 12, 16, 20], [8, 12, 16]
+    shapes = [(int(rng.choice(Bs)), int(rng.choice(Bxs))) for _ in range(args.members)]
+    L, dt = PARAMS['L'], PARAMS['dt']
+    inputs, plans = {}, {}
+    for B, _ in shapes:
+        if B not in inputs:
+            inputs[B] = model_inputs(hp, B, 2, seed=0)
+
+    def plan(B, Bx, prec):
+        pl = hp.Plan(B, Bx, 3, prec, hp.HP_REAL)
+        inp = inputs[B]
+        pl.set_model(L, inp['b'], inp['G'], inp['MR'], inp['gyro'])
+        return pl
+
+    def params(k):
+        r = np.random.default_rng(5000 + k)
+        Q = []
+        for _ in range(2):
+            q, rr = np.linalg.qr(r.standard_normal((3, 3)))
+            q = q * np.sign(np.diag(rr))
+            if np.linalg.det(q) < 0:
+                q[:, 0] = -q[:, 0]
+            Q.append(q)
+        return Q[0], np.sort(r.uniform(5, 20, 3))[::-1], Q[1], r.uniform(-1, 1, 3)
+
+    # per-density FP64 loop (timed on every member, a few steps each)
+    k64 = 3
+    t64 = 0.0
+    ref = {}
+    nsample = 2
+    for key in sorted(set(shapes)):
+        p64 = plan(key[0], key[1], hp.HP_FP64)
+        st = hp.State(p64)
+        for k, sh in enumerate(shapes):
+            if sh != key:
+                continue
+            U, s_, V, mu = params(k)
+            st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
+            st.step(dt, 'euler', 1)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st.step(dt, 'euler', k64)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            t64 += e0.elapsed_time(e1)
+            if k < nsample:
+                st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
+                st.step(dt, 'euler', args.warmup + args.steps)
+                ref[k] = st.store()
+        del st, p64
+    rate64 = args.members * k64 / (t64 / 1e3)
+    # the batch (mixed precision)
+    for key in sorted(set(shapes)):
+        plans[key] = plan(key[0], key[1], hp.HP_MIXED)
+    states = []
+    for k, sh in enumerate(shapes):
+        st = hp.State(plans[sh])
+        U, s_, V, mu = params(k)
+        st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
+        states.append(st)
+    batch = hp.Batch(states)
+    batch.step(dt, 'euler', args.warmup)          # warm-up and graph capture
+    torch.cuda.synchronize(dev)
+    accuracy = None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    batch.step(dt, 'euler', args.steps)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    info = batch.info()
+    errs = [float(np.linalg.norm(states[k].store() - ref[k]) / np.linalg.norm(ref[k])) for k in ref]
+    accuracy = max(errs)
+    rate = args.members * args.steps / (ms / 1e3)
+    hist = {}
+    for B, Bx in shapes:
+        hist[f'B{B}_omega{2 * Bx}^3'] = hist.get(f'B{B}_omega{2 * Bx}^3', 0) + 1
+    out = {'metric': 'batched FP member-steps/s (uneven bandlimits and omega grids)', 'value': round(rate, 2),
+           'unit': 'member-steps/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+           'ms_per_batch_step': round(ms / args.steps, 3), 'host_wall_s': round(wall, 3),
+           'higher_is_better': True, 'dtype': 'f32 (f64 accumulation)', 'data': 'synthetic',
+           'config': {'workload': 'batch of pendulum FP propagation steps (Euler, dt=1e-3)',
+                      'members': args.members, 'shapes': hist, 'distinct_plans': len(plans)},
+           'fp64_per_density_loop': {'value': round(rate64, 2), 'unit': 'member-steps/s', 'steps_each': k64},
+           'speedup_vs_fp64_loop': round(rate / rate64, 3),
+           'graph_launches': info['graph_launches'], 'concurrent_streams': info['streams'],
+           'max_rel_l2_vs_fp64_loop': accuracy}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     return 0
 
 

@@ -43,7 +43,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
-           'hp_state_init_mf_gauss']
+           'hp_state_init_mf_gauss', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info']
 
 
 class HPError(RuntimeError):
@@ -134,6 +134,10 @@ def _load():
         'hp_state_moments': [vp, ctypes.POINTER(hp_moments_t), vp],
         'hp_density_mf_gauss': [vp, vp, vp, vp, vp, vp, vp, ip],
         'hp_state_init_mf_gauss': [vp, vp, vp, vp, vp, vp],
+        'hp_batch_create': [vp, vp, ip, ctypes.POINTER(vp)],
+        'hp_batch_destroy': [vp],
+        'hp_batch_step': [vp, dp, ip, ip],
+        'hp_batch_info': [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ip)],
         'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
     }
     for name, args in sig.items():
@@ -533,6 +537,37 @@ class Collision:
         po, _ = _ptr(out, np.float64)
         _check(_lib.hp_collision_df(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(po), mf))
         return out
+
+
+class Batch:
+    """Independent densities advanced together: member states of any plans
+    (uneven bandlimits and omega grids), each optionally with a collision
+    operator (hybrid step).  Members on different plans run concurrently; the
+    steps are replayed from a CUDA graph after one warm-up step."""
+
+    def __init__(self, states, collisions=None):
+        n = len(states)
+        self._states = list(states)
+        self._colls = list(collisions) if collisions is not None else [None] * n
+        arr = (ctypes.c_void_p * n)(*[st._h for st in self._states])
+        carr = (ctypes.c_void_p * n)(*[c._h if c is not None else None for c in self._colls])
+        h = ctypes.c_void_p()
+        _check(_lib.hp_batch_create(arr, carr, n, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h is not None and _lib is not None:
+            _lib.hp_batch_destroy(h)
+            self._h = None
+
+    def step(self, dt: float, method: str = 'euler', nsteps: int = 1):
+        _check(_lib.hp_batch_step(self._h, float(dt), METHODS[method.lower()], int(nsteps)))
+
+    def info(self) -> dict:
+        g, s = ctypes.c_longlong(), ctypes.c_int()
+        _check(_lib.hp_batch_info(self._h, ctypes.byref(g), ctypes.byref(s)))
+        return dict(graph_launches=g.value, streams=s.value)
 
 
 @lru_cache(maxsize=32)

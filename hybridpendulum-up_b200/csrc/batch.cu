@@ -1,0 +1,214 @@
+// Batched propagation: many independent densities (each its own resident
+// state, of any bandlimit and omega grid) advance together.  Members whose
+// plans differ run concurrently on their own streams; members that share a
+// plan (and so its workspace) run one after the other on that plan's stream.
+// After one eager warm-up step (which sizes every workspace), two steps of the
+// whole batch are captured into one CUDA graph and replayed: the state
+// buffers ping-pong with period two for every method, so a two-step graph
+// starts and ends on the same buffers.  An odd remainder runs eagerly.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "plan.hpp"
+
+extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps);
+extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int method, int nsteps);
+extern "C" int hp_plan_set_stream(hp_plan* p, void* stream);
+
+struct hp_batch {
+  std::vector<hp_state*> st;
+  std::vector<hp_collision*> coll;
+  std::vector<hp_plan*> plans;              // distinct plans
+  std::vector<int> plan_of;                 // member -> index in plans
+  std::vector<cudaStream_t> streams;        // one per distinct plan
+  std::vector<cudaStream_t> saved;          // the plans' own streams
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double dt = 0.0;
+  int method = -1;
+  std::vector<double2*> capF;               // each member's F at capture
+  long long graph_launches = 0;
+};
+
+namespace {
+
+#define BT_CHECK(expr)          \
+  do {                          \
+    int _s = (expr);            \
+    if (_s != HP_OK) return _s; \
+  } while (0)
+
+void drop_graph(hp_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int use_streams(hp_batch* b, bool on) {
+  for (size_t i = 0; i < b->plans.size(); ++i)
+    BT_CHECK(hp_plan_set_stream(b->plans[i], on ? (void*)b->streams[i] : (void*)b->saved[i]));
+  return HP_OK;
+}
+
+int member_step(hp_batch* b, size_t i, double dt, int method) {
+  return b->coll[i] ? hp_state_hybrid_step(b->st[i], b->coll[i], dt, method, 1)
+                    : hp_state_step(b->st[i], dt, method, 1);
+}
+
+// one step of every member, forked from `origin` and joined back into it
+int batch_step(hp_batch* b, double dt, int method) {
+  HP_CUDA_TRY(cudaEventRecord(b->fork, b->origin));
+  for (auto s : b->streams) HP_CUDA_TRY(cudaStreamWaitEvent(s, b->fork, 0));
+  for (size_t i = 0; i < b->st.size(); ++i) BT_CHECK(member_step(b, i, dt, method));
+  for (size_t k = 0; k < b->streams.size(); ++k) {
+    HP_CUDA_TRY(cudaEventRecord(b->joins[k], b->streams[k]));
+    HP_CUDA_TRY(cudaStreamWaitEvent(b->origin, b->joins[k], 0));
+  }
+  return HP_OK;
+}
+
+bool at_capture_buffers(const hp_batch* b) {
+  for (size_t i = 0; i < b->st.size(); ++i)
+    if (b->st[i]->F != b->capF[i]) return false;
+  return true;
+}
+
+int capture(hp_batch* b, double dt, int method) {
+  b->capF.clear();
+  for (auto s : b->st) b->capF.push_back(s->F);
+  std::vector<bool> fg(b->st.size());
+  for (size_t i = 0; i < b->st.size(); ++i) fg[i] = b->st[i]->fg_valid;
+  HP_CUDA_TRY(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed));
+  int st = batch_step(b, dt, method);
+  if (st == HP_OK) st = batch_step(b, dt, method);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(b->origin, &g);
+  if (st != HP_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) { hp_set_error(cudaGetErrorString(e)); return HP_ERR_CUDA; }
+  b->graph = g;
+  HP_CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+  // capturing enqueued nothing: the buffers are back where they started
+  for (size_t i = 0; i < b->st.size(); ++i) {
+    if (b->st[i]->F != b->capF[i]) { hp_set_error("state buffers do not cycle with period two"); return HP_ERR_UNSUPPORTED; }
+    b->st[i]->fg_valid = fg[i];
+  }
+  b->dt = dt;
+  b->method = method;
+  return HP_OK;
+}
+
+}  // namespace
+
+extern "C" int hp_batch_create(hp_state* const* states, hp_collision* const* colls, int n, hp_batch** out) {
+  if (!states || n < 1 || !out) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  *out = nullptr;
+  hp_batch* b = new hp_batch();
+  for (int i = 0; i < n; ++i) {
+    if (!states[i]) { delete b; hp_set_error("null state"); return HP_ERR_INVALID; }
+    for (int j = 0; j < i; ++j)
+      if (states[j] == states[i]) { delete b; hp_set_error("a state appears twice in the batch"); return HP_ERR_INVALID; }
+    b->st.push_back(states[i]);
+    b->coll.push_back(colls ? colls[i] : nullptr);
+    hp_plan* p = states[i]->plan;
+    auto it = std::find(b->plans.begin(), b->plans.end(), p);
+    if (it == b->plans.end()) {
+      b->plans.push_back(p);
+      b->plan_of.push_back((int)b->plans.size() - 1);
+    } else {
+      b->plan_of.push_back((int)(it - b->plans.begin()));
+    }
+  }
+  auto fail = [&](cudaError_t e) {
+    hp_set_error(cudaGetErrorString(e));
+    for (auto s : b->streams) cudaStreamDestroy(s);
+    for (auto ev : b->joins) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    delete b;
+    return HP_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  for (auto p : b->plans) {
+    cudaStream_t s;
+    cudaEvent_t ev;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    b->streams.push_back(s);
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+    b->joins.push_back(ev);
+    b->saved.push_back(p->stream);
+  }
+  *out = b;
+  return HP_OK;
+}
+
+extern "C" int hp_batch_destroy(hp_batch* b) {
+  if (!b) return HP_OK;
+  drop_graph(b);
+  for (auto s : b->streams) cudaStreamDestroy(s);
+  for (auto ev : b->joins) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+  return HP_OK;
+}
+
+extern "C" int hp_batch_step(hp_batch* b, double dt, int method, int nsteps) {
+  if (!b || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
+  if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
+  for (auto p : b->plans)
+    if (p->prof_on) { hp_set_error("disable plan profiling before batched steps"); return HP_ERR_INVALID; }
+  if (b->exec && (dt != b->dt || method != b->method)) drop_graph(b);
+  BT_CHECK(use_streams(b, true));
+  int st = HP_OK;
+  int done = 0;
+  if (!b->exec && nsteps >= 3) {
+    st = batch_step(b, dt, method);   // warm-up: every workspace and table exists afterwards
+    ++done;
+    if (st == HP_OK) {
+      const cudaError_t e = cudaStreamSynchronize(b->origin);
+      if (e != cudaSuccess) { hp_set_error(cudaGetErrorString(e)); st = HP_ERR_CUDA; }
+    }
+    if (st == HP_OK) st = capture(b, dt, method);
+  }
+  if (st == HP_OK && b->exec) {
+    if (!at_capture_buffers(b) && nsteps - done >= 1) {
+      st = batch_step(b, dt, method);
+      ++done;
+    }
+    while (st == HP_OK && nsteps - done >= 2 && at_capture_buffers(b)) {
+      const cudaError_t e = cudaGraphLaunch(b->exec, b->origin);
+      if (e != cudaSuccess) { hp_set_error(cudaGetErrorString(e)); st = HP_ERR_CUDA; break; }
+      ++b->graph_launches;
+      done += 2;
+    }
+  }
+  while (st == HP_OK && done < nsteps) {
+    st = batch_step(b, dt, method);
+    ++done;
+  }
+  // the hybrid members' resident densities are valid after any full step
+  if (st == HP_OK && nsteps > 0)
+    for (size_t i = 0; i < b->st.size(); ++i)
+      if (b->coll[i]) b->st[i]->fg_valid = true;
+  const cudaError_t e = cudaStreamSynchronize(b->origin);
+  const int rs = use_streams(b, false);
+  if (st != HP_OK) return st;
+  if (e != cudaSuccess) { hp_set_error(cudaGetErrorString(e)); return HP_ERR_CUDA; }
+  return rs;
+}
+
+extern "C" int hp_batch_info(hp_batch* b, long long* graph_launches, int* concurrent_streams) {
+  if (!b) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (graph_launches) *graph_launches = b->graph_launches;
+  if (concurrent_streams) *concurrent_streams = (int)b->streams.size();
+  return HP_OK;
+}

@@ -18,6 +18,14 @@ extern "C" const char* hp_last_error(void) { return g_err.c_str(); }
     if (_s != HP_OK) return _s;     \
   } while (0)
 
+void hp_plan::ws_release(const char* name) {
+  for (auto& kv : ws)
+    if (kv.first == name && kv.second.p) {
+      cudaFree(kv.second.p);
+      kv.second = Buf{};
+    }
+}
+
 void* hp_plan::ws_get(const char* name, size_t bytes, int* status) {
   for (auto& kv : ws) {
     if (kv.first == name) {
@@ -508,7 +516,8 @@ extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
   hp_state* s = new hp_state();
   s->plan = p;
   const size_t ib = 16 * (size_t)p->nrows * p->nx;
-  double2** bufs[4] = {&s->F, &s->F2, &s->F3, &s->acc};
+  // F3 and acc are allocated on first use by a method that needs them
+  double2** bufs[2] = {&s->F, &s->F2};
   for (auto b : bufs) {
     if (cudaMalloc(b, ib) != cudaSuccess) {
       cudaGetLastError();
@@ -556,10 +565,24 @@ extern "C" int hp_state_store(hp_state* s, double* F, int mem) {
   return HP_OK;
 }
 
+// stage buffers of the midpoint and Runge-Kutta methods, allocated on first use
+static int state_bufs(hp_state* s, int method) {
+  const size_t ib = 16 * (size_t)s->plan->nrows * s->plan->nx;
+  if (method != HP_EULER && !s->F3) {
+    if (cudaMalloc(&s->F3, ib) != cudaSuccess) { cudaGetLastError(); s->F3 = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
+  }
+  if ((method == HP_RK2 || method == HP_RK4) && !s->acc) {
+    if (cudaMalloc(&s->acc, ib) != cudaSuccess) { cudaGetLastError(); s->acc = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
+  }
+  return HP_OK;
+}
+
 extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
   if (!s || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
   hp_plan* p = s->plan;
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
+  if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
+  HP_CHECK(state_bufs(s, method));
   if (nsteps > 0) s->fg_valid = false;
   for (int k = 0; k < nsteps; ++k) HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
   return HP_OK;
@@ -575,6 +598,7 @@ extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int
   if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
   if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
   cudaStream_t st = p->stream;
+  HP_CHECK(state_bufs(s, method));
   if (!s->fg) {
     const size_t eb = p->precision == HP_FP64 ? sizeof(double) : sizeof(float);
     if (cudaMalloc(&s->fg, eb * (size_t)p->n_grid()) != cudaSuccess) {

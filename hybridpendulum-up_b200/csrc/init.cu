@@ -180,5 +180,7 @@ extern "C" int hp_state_init_mf_gauss(hp_state* sta, const double* U, const doub
   if (st) return st;
   sta->fg_valid = false;
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  // the FP64 grid density and transform buffers are only needed here
+  for (const char* k : {"init.f", "tf.t1", "tf.t2"}) p->ws_release(k);
   return HP_OK;
 }

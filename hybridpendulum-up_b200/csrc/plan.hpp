@@ -69,6 +69,7 @@ struct hp_plan {
   // workspace (grow-only), keyed by name
   std::vector<std::pair<std::string, Buf>> ws;
   void* ws_get(const char* name, size_t bytes, int* status);
+  void ws_release(const char* name);   // frees a workspace buffer (re-created on demand)
 
   RowLayout layout() const {
     RowLayout L;

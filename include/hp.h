@@ -240,6 +240,22 @@ int hp_density_mf_gauss(hp_plan* plan, const double* U, const double* s, const d
 int hp_state_init_mf_gauss(hp_state* state, const double* U, const double* s, const double* V,
                            const double* mu, const double* Sigma);
 
+/* ---- batches: independent densities advanced together (config 5 of the
+ * build's workloads; no counterpart in the reference, whose drivers loop over
+ * one density) ----
+ * Members are resident states of any plans (bandlimit, omega grid, precision);
+ * colls (may be NULL, or NULL entries) makes a member's step the hybrid step.
+ * Members on different plans run concurrently on the batch's streams; members
+ * sharing a plan share its workspace and run in turn.  hp_batch_step runs one
+ * eager warm-up step, then replays a CUDA graph of two batch steps; the graph
+ * is rebuilt when dt or method change.  Plan profiling must be off. */
+typedef struct hp_batch hp_batch;
+int hp_batch_create(hp_state* const* states, hp_collision* const* colls, int n, hp_batch** batch);
+int hp_batch_destroy(hp_batch* batch);
+int hp_batch_step(hp_batch* batch, double dt, int method, int nsteps);
+/* graph replays so far and the number of concurrent streams */
+int hp_batch_info(hp_batch* batch, long long* graph_launches, int* concurrent_streams);
+
 /* ---- statistics: the raw moments of get_stat (propagation/pendulum.m:547-594,
  * pendulum_reduced_hybrid.m:304-351) ----
  * The moments are computed from the coefficients (F^l_mn with l <= 2 at the
