@@ -132,6 +132,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   constexpr int NM = CPLX ? D : B;
   constexpr int MLO = CPLX ? -lmax : 0;
   constexpr int NPAIR = NM * D;
+  // G/H stride per (bb, m): 2B q-bins x P omega points, padded by P so that
+  // the P-wide groups of the gamma stage fall on distinct banks
+  constexpr int GS = NB2 * P + P;
+  // real staging: runs of NB*2B values in slots of RS elements (a multiple of
+  // the RSB elements that span the 32 banks)
+  constexpr int RSB = 128 / (int)sizeof(T);
+  constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nrows = (int)L.nrows;
   T* sd = reinterpret_cast<T*>(smraw);
@@ -193,7 +200,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
       }
 #pragma unroll
       for (int bb = 0; bb < NB; ++bb) {
-        C* g = sG + ((bb * NM + mi) * NB2) * P + p;
+        C* g = sG + (bb * NM + mi) * GS + p;
         g[q * P] = acc[bb];
         if (pe.y >> 24) g[B * P] = czero<C>();
       }
@@ -201,7 +208,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
     __syncthreads();
     // gamma stage: item (bb, mi, p): FFT over n -> c, in place
     for (int it = tid; it < NB * NM * P; it += nth) {
-      C* g = sG + (it / P) * NB2 * P + it % P;
+      C* g = sG + (it / P) * GS + it % P;
       C x[NB2];
 #pragma unroll
       for (int j = 0; j < NB2; ++j) x[j] = g[j * P];
@@ -219,14 +226,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
     const int p = tid % P, c = (tid / P) % NCOL, bb = tid / (P * NCOL);
     C x[NB2];
     if (act) {
-      const C* h = sG + (bb * NM * NB2 + c) * P + p;
+      const C* h = sG + bb * NM * GS + c * P + p;
 #pragma unroll
       for (int q = 0; q < NB2; ++q) x[q] = czero<C>();
       if (CPLX) {
 #pragma unroll
         for (int mi = 0; mi < NM; ++mi) {
           const int m = mi + MLO;
-          x[m >= 0 ? m : m + NB2] = h[mi * NB2 * P];
+          x[m >= 0 ? m : m + NB2] = h[mi * GS];
         }
       } else {
         const C* h2 = h + B * P;   // column c + B
@@ -237,7 +244,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
         }
 #pragma unroll
         for (int m = 1; m < B; ++m) {
-          const C u = h[m * NB2 * P], v = h2[m * NB2 * P];
+          const C u = h[m * GS], v = h2[m * GS];
           // z[m] = u + i v ; z[N-m] = conj(u) + i conj(v)
           x[m].x = u.x - v.y;
           x[m].y = u.y + v.x;
@@ -254,11 +261,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
       } else {
-        // runs of NB*2B values per (p, c) padded by one element: consecutive
-        // threads of a warp then write distinct banks
-        constexpr int RS = NB * NB2 + 1;
-        T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS + bb * NB2;
-        T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS + bb * NB2;
+        // runs of NB*2B values per (p, c) padded by one element
+        constexpr int RS1 = NB * NB2 + 1;
+        T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS1 + bb * NB2;
+        T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS1 + bb * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) {
           st[a] = x[a].x;
@@ -461,11 +467,13 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr int NM = CPLX ? 2 * B - 1 : B;
   static constexpr int NCOL = CPLX ? 2 * B : B;
   static constexpr long long bytes(int nb, int p) {
-    const long long g = (long long)NM * 2 * B * 2 * (long long)sizeof(T);            // G/H, complex
-    const long long st = CPLX ? (long long)2 * B * 2 * B * 2 * (long long)sizeof(T)  // f staging
-                              : (long long)2 * B * (2 * B + 1) * (long long)sizeof(T);  // (runs padded by 1 per nb)
-    return nb * nrows * (long long)sizeof(T) + 32 + (long long)NM * (2 * B - 1) * 8 +
-           (long long)nb * p * (g > st ? g : st);
+    const long long c = 2 * (long long)sizeof(T);
+    const long long g = (long long)nb * NM * (2 * B * p + p) * c;                     // G/H, padded
+    const long long rsb = 128 / (long long)sizeof(T);
+    const long long rs = ((long long)nb * 2 * B + rsb - 1) / rsb * rsb + 1;
+    const long long st = CPLX ? (long long)p * 2 * B * nb * 2 * B * c                 // f staging
+                              : (long long)p * 2 * B * rs * (long long)sizeof(T);
+    return nb * nrows * (long long)sizeof(T) + 32 + (long long)NM * (2 * B - 1) * 8 + (g > st ? g : st);
   }
   // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB)
   static constexpr long long budget() { return bytes(1, 4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
@@ -491,9 +499,11 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   constexpr int NB = Cfg::NB, P = Cfg::P, NB2 = 2 * B, NM = Cfg::NM;
   static_assert(NB * Cfg::NCOL * P <= 256, "alpha stage must fit one round");
   const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
-  const size_t sg_bytes = std::max((size_t)NB * NM * NB2 * P * sizeof(C),
+  constexpr int RSB = 128 / (int)sizeof(T);
+  constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
+  const size_t sg_bytes = std::max((size_t)NB * NM * (NB2 * P + P) * sizeof(C),
                                    CPLX ? (size_t)P * NB2 * NB * NB2 * sizeof(C)
-                                        : (size_t)P * NB2 * (NB * NB2 + 1) * sizeof(T));
+                                        : (size_t)P * NB2 * RS * sizeof(T));
   constexpr int NPAIR = NM * (2 * B - 1);
   const size_t pr_bytes = ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16;
   const size_t smem = sd_bytes + pr_bytes + sg_bytes;
