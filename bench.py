@@ -48,8 +48,9 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--fp64-steps', type=int, default=None)
-    ap.add_argument('--workload', default='step', choices=['step', 'batch'],
-                    help='step: the headline FP step; batch: uneven-bandlimit batch of densities')
+    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform'],
+                    help='step: the headline FP step; batch: uneven-bandlimit batch of densities; '
+                         'transform: B=32 round-trip precision stress')
     ap.add_argument('--members', type=int, default=64)
     return ap.parse_args()
 
@@ -272,6 +273,8 @@ def main():
 
     if args.workload == 'batch':
         return bench_batch(args, rank, world, local)
+    if args.workload == 'transform':
+        return bench_transform(args, rank, local)
     if args.impl == 'reference':
         if rank != 0:
             return 0
@@ -570,6 +573,78 @@ def bench_batch(args, rank, world, local):
            'max_rel_l2_vs_fp64_loop': accuracy}
     if rank == 0:
         print(json.dumps(out), flush=True)
+    return 0
+
+
+def bench_transform(args, rank, local):
+    """ifftSO3R -> fftSO3R round trip at B=32 (64^3 Euler grid) on a 24^3 omega
+    grid, complex coefficients i.i.d. N(0,1)/(2l+1) per degree (seeded), in FP64
+    and in mixed precision; errors are relative L2 against the input (the FP64
+    round trip is the identity up to rounding) and against the FP64 density.
+    Prints one JSON line (not the headline)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    hp = importlib.import_module('hybridpendulum-up_b200')
+    B, Bx = 32, 12
+    lmax = B - 1
+    D = 2 * lmax + 1
+    N = 2 * Bx
+    g = torch.Generator(device=dev).manual_seed(7 + rank)
+    shape = (N, N, N, lmax + 1, D, D)        # reversed MATLAB order, C-contiguous
+    F = torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
+                      torch.randn(shape, generator=g, device=dev, dtype=torch.float64))
+    l = torch.arange(lmax + 1, device=dev).view(1, 1, 1, -1, 1, 1)
+    m = (torch.arange(D, device=dev) - lmax).view(1, 1, 1, 1, 1, -1)
+    n = (torch.arange(D, device=dev) - lmax).view(1, 1, 1, 1, -1, 1)
+    F = F * ((m.abs() <= l) & (n.abs() <= l)) / (2 * l + 1)
+    F = F.contiguous()
+    nF = torch.linalg.vector_norm(F).item()
+    out = {}
+    fsample = None
+    ns = (2 * B) ** 3 * N * N * 2            # first two omega planes of the density
+    for name, prec in (('fp64', hp.HP_FP64), ('mixed', hp.HP_MIXED)):
+        plan = hp.Plan(B, Bx, 3, prec, hp.HP_COMPLEX)
+        st = hp.State(plan)
+        cdt = torch.complex128 if prec == hp.HP_FP64 else torch.complex64
+        f = torch.empty((2 * B) ** 3 * N ** 3, dtype=cdt, device=dev)
+        st.load(F)
+        st.density_into(f.data_ptr())
+        st.load_density(f.data_ptr())
+        torch.cuda.synchronize(dev)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        st.load(F)
+        torch.cuda.synchronize(dev)
+        e[0].record()
+        st.density_into(f.data_ptr())
+        e[1].record()
+        st.load_density(f.data_ptr())
+        e[2].record()
+        torch.cuda.synchronize(dev)
+        r = {'backward_ms': round(e[0].elapsed_time(e[1]), 2), 'forward_ms': round(e[1].elapsed_time(e[2]), 2)}
+        if fsample is None:
+            fsample = f[:ns].clone()
+        else:
+            r['density_rel_l2_vs_fp64'] = (torch.linalg.vector_norm(f[:ns].to(torch.complex128) - fsample) /
+                                           torch.linalg.vector_norm(fsample)).item()
+        del f
+        torch.cuda.empty_cache()
+        F2 = torch.empty_like(F)
+        st.store(F2)
+        r['round_trip_rel_l2'] = (torch.linalg.vector_norm(F2 - F) / nF).item()
+        del F2
+        out[name] = r
+        del st, plan
+        torch.cuda.empty_cache()
+    line = {'metric': 'fftSO3R round trip at B=32, omega 24^3 (complex coefficients)', 'unit': 'ms',
+            'value': round(out['mixed']['backward_ms'] + out['mixed']['forward_ms'], 2), 'higher_is_better': False,
+            'n_gpus': 1, 'dtype': 'f32 (mixed) and f64', 'data': 'synthetic',
+            'config': {'workload': 'transform precision stress', 'B': B, 'omega_grid': '24^3',
+                       'coefficients': 'i.i.d. N(0,1)/(2l+1), complex'},
+            'fp64': out['fp64'], 'mixed': out['mixed'],
+            'not_built': 'TF32-split and BF16x3-split tensor-core beta contractions'}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 

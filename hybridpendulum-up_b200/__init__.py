@@ -43,7 +43,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
-           'hp_state_init_mf_gauss', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info']
+           'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info']
 
 
 class HPError(RuntimeError):
@@ -134,6 +134,7 @@ def _load():
         'hp_state_moments': [vp, ctypes.POINTER(hp_moments_t), vp],
         'hp_density_mf_gauss': [vp, vp, vp, vp, vp, vp, vp, ip],
         'hp_state_init_mf_gauss': [vp, vp, vp, vp, vp, vp],
+        'hp_state_load_density': [vp, vp],
         'hp_batch_create': [vp, vp, ip, ctypes.POINTER(vp)],
         'hp_batch_destroy': [vp],
         'hp_batch_step': [vp, dp, ip, ip],
@@ -466,6 +467,10 @@ class State:
 
     def density_into(self, dev_ptr: int):
         _check(_lib.hp_state_density(self._h, ctypes.c_void_p(dev_ptr)))
+
+    def load_density(self, dev_ptr: int):
+        """F = fftSO3R(f) from a device density in the plan's compute precision."""
+        _check(_lib.hp_state_load_density(self._h, ctypes.c_void_p(dev_ptr)))
 
     def normalize(self, mass: float) -> float:
         """Scale the state so its l = 0 mass is `mass`; returns the factor."""

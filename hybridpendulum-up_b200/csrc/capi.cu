@@ -588,6 +588,18 @@ extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
   return HP_OK;
 }
 
+// Loads the state from a grid density on the device in the plan's compute
+// precision (double for HP_FP64, float for HP_MIXED; complex interleaved for
+// HP_COMPLEX plans): F = fftSO3R(f).
+extern "C" int hp_state_load_density(hp_state* s, const void* f) {
+  if (!s || !f) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  hp_plan* p = s->plan;
+  HP_CHECK(hp_forward_internal(p, f, p->symmetry == HP_COMPLEX, s->F, p->stream));
+  s->fg_valid = false;
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}
+
 // pendulum_reduced_hybrid.m:226-234 per step: F = propagate_den(F, f);
 // f = backward(F); f += dt * df(f); F = forward(f).
 extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int method, int nsteps) {

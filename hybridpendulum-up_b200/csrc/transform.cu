@@ -123,7 +123,10 @@ __device__ __forceinline__ void store16(double* dst, const double* s) {
 // are read in the [row][omega] layout with the P omega points of a batch on
 // consecutive lanes, so every coefficient load is coalesced; the per-(omega,
 // beta) intermediates G -> H live in shared memory as [bb][m][q][p].
-template <int B, typename T, int NB, int P, bool CPLX>
+// GD: the (2l+1) d table of the block's betas is read from a global table
+// [group][row][NB] (large bandlimits, where it does not fit shared memory)
+// instead of being staged from the d table `wig`.
+template <int B, typename T, int NB, int P, bool CPLX, bool GD>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
                                                   const T* __restrict__ wig, const int2* __restrict__ pairs,
                                                   void* __restrict__ fout, int nbatch) {
@@ -141,8 +144,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nrows = (int)L.nrows;
-  T* sd = reinterpret_cast<T*>(smraw);
-  int2* spairs = reinterpret_cast<int2*>(smraw + ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16);
+  T* sds = reinterpret_cast<T*>(smraw);
+  int2* spairs = reinterpret_cast<int2*>(smraw + (GD ? 0 : ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16));
   C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
   // beta groups of one omega chunk are consecutive blocks, so they read the
   // same coefficient rows close together in time (L2 reuse)
@@ -152,10 +155,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   const int b0 = grp * NB;
   const int nbv = min(NB, NB2 - b0);
   const int tid = threadIdx.x, nth = blockDim.x;
-  for (int e = tid; e < NB * nrows; e += nth) {   // interleaved [row][bb]
+  const T* sd = GD ? wig + (size_t)grp * nrows * NB : sds;
+  for (int e = tid; !GD && e < NB * nrows; e += nth) {   // interleaved [row][bb]
     const int r = e / NB, bb = e % NB;
     const T l2 = (T)(2 * L.rows[r].x + 1);
-    sd[e] = (bb < nbv) ? l2 * wig[(size_t)(b0 + bb) * nrows + r] : (T)0;
+    sds[e] = (bb < nbv) ? l2 * wig[(size_t)(b0 + bb) * nrows + r] : (T)0;
   }
   for (int e = tid; e < NPAIR; e += nth) spairs[e] = pairs[e];
   const long long nx = L.nx;
@@ -306,7 +310,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
 //   gamma stage  Q[m][n]  = sum_c Q1[c][m] e^{+i n gamma_c}
 //   beta  stage  Fa[w][(m,n,l)] += sum_b w_b d^l_mn(beta_b) Q_b[m][n]
 // The beta sum over groups of betas is accumulated with atomics.
-template <int B, typename T, int NB, bool CPLX>
+// GD: w_b d of the block's betas from a global table [group][NB][row]
+// (large bandlimits) instead of staging it from the d table `wig`.
+template <int B, typename T, int NB, bool CPLX, bool GD>
 __global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restrict__ fin,
                                               const T* __restrict__ wig, const double* __restrict__ qw,
                                               const double* __restrict__ mult,
@@ -316,17 +322,18 @@ __global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restric
   constexpr int NM = CPLX ? D : B;
   constexpr int MLO = CPLX ? -lmax : 0;
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* sd = reinterpret_cast<T*>(smraw);  // [NB][nrows] w_b d
-  size_t off = ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
+  T* sds = reinterpret_cast<T*>(smraw);  // [NB][nrows] w_b d
+  const T* sd = GD ? wig + (size_t)blockIdx.y * NB * L.nrows : sds;
+  size_t off = GD ? 0 : ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
   C* sQ = reinterpret_cast<C*>(smraw + off);  // [P][NB][NM][NB2] (n bins)
   size_t off2 = off + (size_t)P * NB * NM * NB2 * sizeof(C);
   C* sIn = reinterpret_cast<C*>(smraw + off2);  // [P][NB][NB2 (c)][NB2 (a)]
   const int b0 = blockIdx.y * NB;
   const int nbv = min(NB, NB2 - b0);
   const int tid = threadIdx.x, nth = blockDim.x;
-  for (long long e = tid; e < (long long)NB * L.nrows; e += nth) {
+  for (long long e = tid; !GD && e < (long long)NB * L.nrows; e += nth) {
     const int bb = (int)(e / L.nrows);
-    sd[e] = (bb < nbv) ? (T)(qw[b0 + bb] * (double)wig[(long long)(b0 + bb) * L.nrows + e % L.nrows]) : (T)0;
+    sds[e] = (bb < nbv) ? (T)(qw[b0 + bb] * (double)wig[(long long)(b0 + bb) * L.nrows + e % L.nrows]) : (T)0;
   }
   const long long wbeg = blockIdx.x * w_per_block;
   const long long wend = min(wbeg + w_per_block, L.nx);
@@ -466,6 +473,8 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
                                           : (long long)B * (B + 1) * (4 * B - 1) / 6;
   static constexpr int NM = CPLX ? 2 * B - 1 : B;
   static constexpr int NCOL = CPLX ? 2 * B : B;
+  // the d table of one beta above 64 KB: read it from a global table
+  static constexpr bool GD = nrows * (long long)sizeof(T) > 64 * 1024;
   static constexpr long long bytes(int nb, int p) {
     const long long c = 2 * (long long)sizeof(T);
     const long long g = (long long)nb * NM * (2 * B * p + p) * c;                     // G/H, padded
@@ -473,7 +482,7 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
     const long long rs = ((long long)nb * 2 * B + rsb - 1) / rsb * rsb + 1;
     const long long st = CPLX ? (long long)p * 2 * B * nb * 2 * B * c                 // f staging
                               : (long long)p * 2 * B * rs * (long long)sizeof(T);
-    return nb * nrows * (long long)sizeof(T) + 32 + (long long)NM * (2 * B - 1) * 8 + (g > st ? g : st);
+    return (GD ? 0 : nb * nrows * (long long)sizeof(T)) + 32 + (long long)NM * (2 * B - 1) * 8 + (g > st ? g : st);
   }
   // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB)
   static constexpr long long budget() { return bytes(1, 4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
@@ -492,13 +501,33 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr int P = pick_p();
 };
 
+template <typename T>
+__global__ void k_sd_table(RowLayout L, const T* __restrict__ wig, T* __restrict__ out, int NB, int ngroups,
+                           int synth, const double* __restrict__ qw = nullptr) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)ngroups * L.nrows * NB;
+  if (t >= n) return;
+  int bb;
+  long long r;
+  if (synth) { bb = (int)(t % NB); r = (t / NB) % L.nrows; }
+  else { r = t % L.nrows; bb = (int)((t / L.nrows) % NB); }
+  const int g = (int)(t / ((long long)NB * L.nrows));
+  const int b = g * NB + bb;
+  T v = (T)0;
+  if (b < 2 * L.B)
+    v = synth ? (T)(2 * L.rows[r].x + 1) * wig[(size_t)b * L.nrows + r]
+              : (T)(qw[b] * (double)wig[(size_t)b * L.nrows + r]);
+  out[t] = v;
+}
+
 template <int B, typename T, bool CPLX>
 static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   using C = c2<T>;
   using Cfg = SynthCfg<B, T, CPLX>;
   constexpr int NB = Cfg::NB, P = Cfg::P, NB2 = 2 * B, NM = Cfg::NM;
+  constexpr bool GD = Cfg::GD;
   static_assert(NB * Cfg::NCOL * P <= 256, "alpha stage must fit one round");
-  const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
+  const size_t sd_bytes = GD ? 0 : ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
   constexpr int RSB = 128 / (int)sizeof(T);
   constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
   const size_t sg_bytes = std::max((size_t)NB * NM * (NB2 * P + P) * sizeof(C),
@@ -541,18 +570,29 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
     HP_CUDA_TRY(cudaMemcpy(dpairs, h.data(), sizeof(int2) * NPAIR, cudaMemcpyHostToDevice));
   }
   const int ngroups = (NB2 + NB - 1) / NB;
+  const T* dtab = sizeof(T) == 8 ? (const T*)(const void*)p->wig64 : (const T*)(const void*)p->wig32;
+  if (GD) {   // (2l+1) d as [group][row][NB], built once per plan
+    const char* gkey = sizeof(T) == 8 ? (CPLX ? "tf.sdg64c" : "tf.sdg64") : (CPLX ? "tf.sdg32c" : "tf.sdg32");
+    bool hv = false;
+    for (auto& kv : p->ws) if (kv.first == gkey) hv = true;
+    const long long n = (long long)ngroups * p->nrows * NB;
+    T* sdg = (T*)p->ws_get(gkey, sizeof(T) * n, &st);
+    if (st) return st;
+    if (!hv) {
+      k_sd_table<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), dtab, sdg, NB, ngroups, 1);
+      HP_CUDA_TRY(cudaGetLastError());
+    }
+    dtab = sdg;
+  }
   const long long nbatches = (p->nx + P - 1) / P;
   // about 8 resident waves of blocks over 148 SMs
   long long gx = std::max(1LL, (148LL * 2 * 8) / ngroups);
   int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
   gx = (nbatches + nbatch - 1) / nbatch;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)(gx * ngroups), 1);
   ProfScope _ps(p, "tf.synth", s);
-  k_synth<B, T, NB, P, CPLX><<<grid, 256, smem, s>>>(p->layout(), Fp,
-                                                     sizeof(T) == 8 ? (const T*)(const void*)p->wig64
-                                                                             : (const T*)(const void*)p->wig32,
-                                                     dpairs, f, nbatch);
+  k_synth<B, T, NB, P, CPLX, GD><<<grid, 256, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
@@ -560,10 +600,13 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
 template <int B, typename T, bool CPLX>
 static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
   using C = c2<T>;
-  constexpr int NB = TfCfg<T>::NB, NB2 = 2 * B;
+  // fewer betas per block at the largest bandlimit (the per-omega tiles grow as B^2)
+  constexpr int NB = B >= 32 ? (sizeof(T) == 8 ? 1 : 2) : TfCfg<T>::NB, NB2 = 2 * B;
   constexpr int NM = CPLX ? 2 * B - 1 : B;
+  constexpr long long NROWS = CPLX ? (long long)B * (2 * B - 1) * (2 * B + 1) / 3 : (long long)B * (B + 1) * (4 * B - 1) / 6;
+  constexpr bool GD = NB * NROWS * (long long)sizeof(T) > 64 * 1024;
   const int threads = TfCfg<T>::threads;
-  const size_t sd_bytes = ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
+  const size_t sd_bytes = GD ? 0 : ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
   const size_t per_p = (size_t)NB * NM * NB2 * sizeof(C) + (size_t)NB * NB2 * NB2 * sizeof(C);
   const int lim = smem_limit();
   int P = 4;
@@ -574,18 +617,30 @@ static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa,
   }
   const size_t smem = sd_bytes + P * per_p;
   const int ngroups = (NB2 + NB - 1) / NB;
+  const T* dtab = sizeof(T) == 8 ? (const T*)(const void*)p->wig64 : (const T*)(const void*)p->wig32;
+  if (GD) {   // w_b d as [group][NB][row], built once per plan
+    int st = HP_OK;
+    const char* gkey = sizeof(T) == 8 ? (CPLX ? "tf.sda64c" : "tf.sda64") : (CPLX ? "tf.sda32c" : "tf.sda32");
+    bool hv = false;
+    for (auto& kv : p->ws) if (kv.first == gkey) hv = true;
+    const long long n = (long long)ngroups * p->nrows * NB;
+    T* sdg = (T*)p->ws_get(gkey, sizeof(T) * n, &st);
+    if (st) return st;
+    if (!hv) {
+      k_sd_table<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), dtab, sdg, NB, ngroups, 0, p->qw);
+      HP_CUDA_TRY(cudaGetLastError());
+    }
+    dtab = sdg;
+  }
   long long wblocks = std::max(1LL, std::min(p->nx, 8LL * 148 * 2 / ngroups + 1));
   long long wpb = (p->nx + wblocks - 1) / wblocks;
   wpb = (wpb + P - 1) / P * P;
   wblocks = (p->nx + wpb - 1) / wpb;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_anal<B, T, NB, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_anal<B, T, NB, CPLX, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)wblocks, (unsigned)ngroups);
   HP_CUDA_TRY(cudaMemsetAsync(Fa, 0, sizeof(C) * p->nrows * p->nx, s));
   ProfScope _ps(p, "tf.anal", s);
-  k_anal<B, T, NB, CPLX><<<grid, threads, smem, s>>>(p->layout(), f,
-                                                      sizeof(T) == 8 ? (const T*)(const void*)p->wig64
-                                                                              : (const T*)(const void*)p->wig32,
-                                                      p->qw, mult, Fa, P, wpb);
+  k_anal<B, T, NB, CPLX, GD><<<grid, threads, smem, s>>>(p->layout(), f, dtab, p->qw, mult, Fa, P, wpb);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }

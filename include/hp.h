@@ -295,6 +295,10 @@ int hp_state_hybrid_step(hp_state* state, hp_collision* coll, double dt, int met
  * for HP_FP64 plans, float for HP_MIXED plans): after hybrid steps the
  * post-collision density f of the last step, otherwise f = ifftSO3R(F). */
 int hp_state_density(hp_state* state, void* f);
+/* The inverse of hp_state_density: loads F = fftSO3R(f) from a device grid
+ * density in the plan's compute precision (fftSO3R_mex('forward',f,d,w),
+ * propagation/mex/sources/fftSO3R/kernel.cu:11-195, without host staging). */
+int hp_state_load_density(hp_state* state, const void* f);
 /* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
 int hp_state_mass(hp_state* state, double* mass);
 /* hp_moments of the resident state; after hybrid steps these are the moments
