@@ -205,6 +205,9 @@ int axis_md(hp_plan* p, const double2* in, double2* out, int axis, double coef, 
     case 20: return axis_md_launch<20>(p, in, out, axis, coef, s);
     case 24: return axis_md_launch<24>(p, in, out, axis, coef, s);
     case 32: return axis_md_launch<32>(p, in, out, axis, coef, s);
+    case 40: return axis_md_launch<40>(p, in, out, axis, coef, s);
+    case 48: return axis_md_launch<48>(p, in, out, axis, coef, s);
+    case 60: return axis_md_launch<60>(p, in, out, axis, coef, s);
     default:
       hp_set_error("omega grid size 2Bx not supported");
       return HP_ERR_UNSUPPORTED;

@@ -27,6 +27,12 @@
 
 using namespace hp;
 
+#define ST_CHECK(expr)          \
+  do {                          \
+    int _s = (expr);            \
+    if (_s != HP_OK) return _s; \
+  } while (0)
+
 #define HP_CHECK_RET(expr)          \
   do {                              \
     int _s = (expr);                \
@@ -469,6 +475,38 @@ template <typename T> static size_t plane_smem(int N, bool p3) {
   return (size_t)planes * N * (N + 1) * sizeof(c2<T>);
 }
 
+
+// k_local with the widest omega tile (32/16/8/4 points) whose group tile and
+// tap weights fit 110 KB of shared memory (the m = 0 group has (lmax+1)^2 rows).
+template <typename T, int W>
+static int local_w_launch(hp_plan* p, const double2* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
+                          cudaStream_t s) {
+  const size_t lsm = local_smem<T>(p, W);
+  dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
+  ProfScope _ps(p, "deriv.local", s);
+  if (p->ndim == 3) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_local<T, W, 3><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, prm);
+  } else {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_local<T, W, 2><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, prm);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+template <typename T>
+static int launch_local(hp_plan* p, const double2* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
+                        cudaStream_t s) {
+  constexpr size_t budget = 110 * 1024;
+  if (sizeof(T) == 4 && local_smem<T>(p, 32) <= budget) return local_w_launch<T, 32>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 16) <= budget) return local_w_launch<T, 16>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 8) <= budget) return local_w_launch<T, 8>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 4) <= (size_t)200 * 1024) return local_w_launch<T, 4>(p, F, G, Gx, prm, s);
+  hp_set_error("gravity pass tiles exceed shared memory for this bandlimit");
+  return HP_ERR_UNSUPPORTED;
+}
+
 template <int N, typename T>
 static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
                        double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
@@ -489,20 +527,7 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
     k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  {
-    constexpr int W = local_w<T>();
-    const size_t lsm = local_smem<T>(p, W);
-    dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
-    ProfScope _ps(p, "deriv.local", s);
-    if (p->ndim == 3) {
-      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 3><<<grid, 256, lsm, s>>>(L, Fev, G, tap_table<T>(p), (const C*)Gx, prm);
-    } else {
-      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 2><<<grid, 256, lsm, s>>>(L, Fev, G, tap_table<T>(p), (const C*)Gx, prm);
-    }
-    HP_CUDA_TRY(cudaGetLastError());
-  }
+  ST_CHECK(launch_local<T>(p, Fev, G, (const C*)Gx, prm, s));
   // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
   constexpr int CT = PlaneCfg<T>::C;
   const char tkey[] = {'d', 'e', 'r', 'i', 'v', '.', 't', 'i', 'l', 'e', 's', (char)('0' + CT), 0};
@@ -532,6 +557,102 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   return HP_OK;
 }
 
+// ------------------------------------- large omega grids (2-D, N >= 40) ----
+// The per-plane kernel's tiles do not fit shared memory beyond N = 32, so the
+// 2-D derivative goes through whole-array omega FFTs:
+//   Fp = IFFT(F);  Z = x1 S + x2 T with S = i/2 (a+ Fp_{n+1} + a- Fp_{n-1}),
+//   T = 1/2 (a- Fp_{n-1} - a+ Fp_{n+1}) (the u_1, u_2 Lie terms), P1 = b1 x1 Fp,
+//   P2 = b2 x2 Fp;  dF = FFT(Z) + D1 FFT(P1) + D2 FFT(P2) + G.
+template <typename T>
+__global__ void k_phys2d(RowLayout L, const c2<T>* __restrict__ Fp, c2<T>* __restrict__ Z, c2<T>* __restrict__ P1,
+                         c2<T>* __restrict__ P2, DerivParams prm) {
+  using C = c2<T>;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * L.nx) return;
+  const long long row = t / L.nx, w = t % L.nx;
+  const int N = L.N;
+  const T Ll = (T)prm.L;
+  const T x1 = -Ll / 2 + Ll * (T)(int)(w % N) / (T)N, x2 = -Ll / 2 + Ll * (T)(int)(w / N) / (T)N;
+  const char4 q = L.rows[row];
+  const int l = q.x, m = q.y, n = q.z;
+  const T lie = (T)prm.lie;
+  const T ap = lie * sqrt((T)((l - n) * (l + n + 1))), am = lie * sqrt((T)((l + n) * (l - n + 1)));
+  const C vp = (n + 1 <= l) ? Fp[row_of(L, l, m, n + 1) * L.nx + w] : czero<C>();
+  const C vm = (n - 1 >= -l) ? Fp[row_of(L, l, m, n - 1) * L.nx + w] : czero<C>();
+  const T h1 = (T)0.5 * x1, h2 = (T)0.5 * x2;
+  C y;
+  y.x = ap * (-h1 * vp.y - h2 * vp.x) + am * (-h1 * vm.y + h2 * vm.x);
+  y.y = ap * (h1 * vp.x - h2 * vp.y) + am * (h1 * vm.x + h2 * vm.y);
+  Z[t] = y;
+  const C f = Fp[t];
+  P1[t] = ((T)prm.b[0] * x1) * f;
+  P2[t] = ((T)prm.b[1] * x2) * f;
+}
+
+template <typename T>
+__global__ void k_combine2d(RowLayout L, const c2<T>* __restrict__ Z, const c2<T>* __restrict__ P1,
+                            const c2<T>* __restrict__ P2, const c2<T>* __restrict__ G,
+                            const double2* __restrict__ F0, double a, double2* __restrict__ out,
+                            double2* __restrict__ acc, double bacc, double tp) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * L.nx) return;
+  const long long w = t % L.nx;
+  const int N = L.N;
+  const double d1 = tp * kappa_first((int)(w % N), N), d2 = tp * kappa_first((int)(w / N), N);
+  const c2<T> z = Z[t], u = P1[t], v = P2[t], g = G[t];
+  // dF = z + i d1 u + i d2 v + g
+  const double dx = (double)z.x - d1 * (double)u.y - d2 * (double)v.y + (double)g.x;
+  const double dy = (double)z.y + d1 * (double)u.x + d2 * (double)v.x + (double)g.y;
+  double2 o = F0 ? F0[t] : make_double2(0.0, 0.0);
+  o.x += a * dx;
+  o.y += a * dy;
+  out[t] = o;
+  if (acc) {
+    double2 c = acc[t];
+    c.x += bacc * dx;
+    c.y += bacc * dy;
+    acc[t] = c;
+  }
+}
+
+template <typename T>
+static int run_deriv_lines(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
+                           double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
+  using C = c2<T>;
+  if (p->ndim != 2) {
+    hp_set_error("the derivative supports omega grids above 32 points per axis in 2-D only");
+    return HP_ERR_UNSUPPORTED;
+  }
+  int st = HP_OK;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  C* G = (C*)p->ws_get("deriv.G", fb, &st);
+  if (st) return st;
+  C* Fp = (C*)p->ws_get("deriv.Fp", fb, &st);
+  if (st) return st;
+  C* Z = (C*)p->ws_get("deriv.Z", fb, &st);
+  if (st) return st;
+  C* P1 = (C*)p->ws_get("deriv.P1", fb, &st);
+  if (st) return st;
+  C* P2 = (C*)p->ws_get("deriv.P2", fb, &st);
+  if (st) return st;
+  ST_CHECK(launch_local<T>(p, Fev, G, (const C*)Gx, prm, s));
+  ST_CHECK(hp_omega_ifft_rows(p, Fev, Fp, s));
+  const long long n = p->nrows * p->nx;
+  const unsigned g = (unsigned)((n + 255) / 256);
+  {
+    ProfScope _ps(p, "deriv.phys", s);
+    k_phys2d<T><<<g, 256, 0, s>>>(p->layout(), Fp, Z, P1, P2, prm);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  ST_CHECK(hp_omega_fft_rows(p, Z, s));
+  ST_CHECK(hp_omega_fft_rows(p, P1, s));
+  ST_CHECK(hp_omega_fft_rows(p, P2, s));
+  ProfScope _ps(p, "deriv.combine", s);
+  k_combine2d<T><<<g, 256, 0, s>>>(p->layout(), Z, P1, P2, G, F0, a, out, acc, bacc, 2.0 * M_PI / prm.L);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 template <typename T>
 static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
                      double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
@@ -544,6 +665,7 @@ static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a
     case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 40: case 48: case 60: return run_deriv_lines<T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     default:
       hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
       return HP_ERR_UNSUPPORTED;
@@ -711,19 +833,7 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
     k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fi, P3, (T)prm.L);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  {
-    constexpr int W = local_w<T>();
-    const size_t lsm = local_smem<T>(p, W);
-    const dim3 lg((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
-    if (p->ndim == 3) {
-      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 3><<<lg, 256, lsm, s>>>(L, Fi, G, tap_table<T>(p), nullptr, prm);
-    } else {
-      HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-      k_local<T, W, 2><<<lg, 256, lsm, s>>>(L, Fi, G, tap_table<T>(p), nullptr, prm);
-    }
-  }
-  HP_CUDA_TRY(cudaGetLastError());
+  ST_CHECK(launch_local<T>(p, Fi, G, (const c2<T>*)nullptr, prm, s));
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)ntiles, p3 ? N : 1);
   if (p3) {

@@ -145,5 +145,8 @@ int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* o
 int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s);
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s);
 int hp_forward_internal64(hp_plan* p, const double* f, double2* Fint, cudaStream_t s);
+// inverse (scaled 1/nx) / forward omega FFT of every row, in the plan's compute precision
+int hp_omega_ifft_rows(hp_plan* p, const double2* in, void* out, cudaStream_t s);
+int hp_omega_fft_rows(hp_plan* p, void* inout, cudaStream_t s);
 int hp_prod_launch(hp_plan* p, const double2* F, const double2* G, double2* FG, int batch,
                    cudaStream_t s);

@@ -27,7 +27,8 @@ template <int N, typename Tin, typename T, bool INV>
 __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, c2<T>* __restrict__ out,
                                                 long long nplanes, T scale) {
   using C = c2<T>;
-  __shared__ C sm[N * (N + 1)];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);   // [N][N+1]
   const long long pl = blockIdx.x;
   if (pl >= nplanes) return;
   const c2<Tin>* src = in + pl * N * N;
@@ -427,25 +428,31 @@ static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaSt
   // in/out [row][nx]; in may equal out only when Tin == T
   const T scale = inv ? (T)1 / (T)p->nx : (T)1;
   const long long nplanes = p->nrows * (p->ndim == 3 ? N : 1);
-  if (p->ndim == 3) {
-    // plane pass (k1,k2) then line pass along k3, scale applied in the line pass
-    {
+  const size_t smem = sizeof(c2<T>) * N * (N + 1);
+  auto plane = [&](T sc) -> int {
     ProfScope _ps(p, "tf.wplane", s);
-    if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
-    else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, (T)1);
+    if (inv) {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc);
+    } else {
+      HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc);
     }
     HP_CUDA_TRY(cudaGetLastError());
+    return HP_OK;
+  };
+  if (p->ndim == 3) {
+    // plane pass (k1,k2) then line pass along k3, scale applied in the line pass
+    int st = plane((T)1);
+    if (st) return st;
     const long long nt = p->nrows * (long long)N * N;
     ProfScope _ps(p, "tf.wline", s);
     if (inv) k_wline<N, T, true><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
     else k_wline<N, T, false><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
-  } else {
-    ProfScope _ps(p, "tf.wplane", s);
-    if (inv) k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
-    else k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, 0, s>>>(in, out, nplanes, scale);
+    HP_CUDA_TRY(cudaGetLastError());
+    return HP_OK;
   }
-  HP_CUDA_TRY(cudaGetLastError());
-  return HP_OK;
+  return plane(scale);
 }
 
 template <typename Tin, typename T>
@@ -459,8 +466,11 @@ static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cu
     case 20: return omega_fft<20, Tin, T>(p, in, out, inv, s);
     case 24: return omega_fft<24, Tin, T>(p, in, out, inv, s);
     case 32: return omega_fft<32, Tin, T>(p, in, out, inv, s);
+    case 40: return omega_fft<40, Tin, T>(p, in, out, inv, s);
+    case 48: return omega_fft<48, Tin, T>(p, in, out, inv, s);
+    case 60: return omega_fft<60, Tin, T>(p, in, out, inv, s);
     default:
-      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      hp_set_error("omega grid size 2Bx not supported (4, 6, 8, 12, 16, 20, 24, 32, 40, 48, 60)");
       return HP_ERR_UNSUPPORTED;
   }
 }
@@ -601,7 +611,7 @@ template <int B, typename T, bool CPLX>
 static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
   using C = c2<T>;
   // fewer betas per block at the largest bandlimit (the per-omega tiles grow as B^2)
-  constexpr int NB = B >= 32 ? (sizeof(T) == 8 ? 1 : 2) : TfCfg<T>::NB, NB2 = 2 * B;
+  constexpr int NB = B >= 24 ? (sizeof(T) == 8 ? 1 : 2) : TfCfg<T>::NB, NB2 = 2 * B;
   constexpr int NM = CPLX ? 2 * B - 1 : B;
   constexpr long long NROWS = CPLX ? (long long)B * (2 * B - 1) * (2 * B + 1) / 3 : (long long)B * (B + 1) * (4 * B - 1) / 6;
   constexpr bool GD = NB * NROWS * (long long)sizeof(T) > 64 * 1024;
@@ -645,7 +655,7 @@ static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa,
   return HP_OK;
 }
 
-#define HP_FOR_EACH_B(X) X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(32)
+#define HP_FOR_EACH_B(X) X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(24) X(30) X(32)
 
 template <typename T, bool CPLX>
 static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
@@ -654,7 +664,7 @@ static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
     HP_FOR_EACH_B(X)
 #undef X
     default:
-      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,32)");
+      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)");
       return HP_ERR_UNSUPPORTED;
   }
 }
@@ -666,7 +676,7 @@ static int anal_any(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cu
     HP_FOR_EACH_B(X)
 #undef X
     default:
-      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,32)");
+      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)");
       return HP_ERR_UNSUPPORTED;
   }
 }
@@ -743,4 +753,16 @@ int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* o
 int hp_forward_internal64(hp_plan* p, const double* f, double2* Fint, cudaStream_t s) {
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   return forward_T<double>(p, f, 0, Fint, s);   // real density, HP_REAL plans
+}
+
+// Omega FFTs of all rows for the derivative's large-grid path (compute precision).
+int hp_omega_ifft_rows(hp_plan* p, const double2* in, void* out, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  if (p->precision == HP_FP64) return omega_fft_any<double, double>(p, in, (double2*)out, true, s);
+  return omega_fft_any<double, float>(p, in, (float2*)out, true, s);
+}
+int hp_omega_fft_rows(hp_plan* p, void* inout, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  if (p->precision == HP_FP64) return omega_fft_any<double, double>(p, (double2*)inout, (double2*)inout, false, s);
+  return omega_fft_any<float, float>(p, (float2*)inout, (float2*)inout, false, s);
 }
