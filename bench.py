@@ -48,9 +48,10 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--fp64-steps', type=int, default=None)
-    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform'],
+    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform', 'hybrid'],
                     help='step: the headline FP step; batch: uneven-bandlimit batch of densities; '
-                         'transform: B=32 round-trip precision stress')
+                         'transform: B=32 round-trip precision stress; hybrid: the loop of '
+                         'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega)')
     ap.add_argument('--members', type=int, default=64)
     return ap.parse_args()
 
@@ -275,6 +276,8 @@ def main():
         return bench_batch(args, rank, world, local)
     if args.workload == 'transform':
         return bench_transform(args, rank, local)
+    if args.workload == 'hybrid':
+        return bench_hybrid(args, rank, local)
     if args.impl == 'reference':
         if rank != 0:
             return 0
@@ -647,6 +650,84 @@ def bench_transform(args, rank, local):
                        'coefficients': 'i.i.d. N(0,1)/(2l+1), complex'},
             'fp64': out['fp64'], 'mixed': out['mixed'],
             'not_built': 'TF32-split and BF16x3-split tensor-core beta contractions'}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_hybrid(args, rank, local):
+    """The time loop of pendulum_reduced_hybrid.m:224-238 at its own sizes and
+    parameters (BR = Bx = 30, L = 3.4, scaled time, wall collision with
+    restitution 0.8, nD = 10; pendulum_reduced_hybrid.m:28-128): per step the
+    density-gravity propagation (Euler), backward transform, collision update,
+    forward transform and the get_stat moments, all on the device.  Prints one
+    JSON line (not the headline)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    hp = importlib.import_module('hybridpendulum-up_b200')
+    B, Bx, L = 30, 30, 3.4
+    J, rho, mass, g = 0.01436, 0.1, 1.0642, 9.8
+    tscale = math.sqrt(J / (mass * g * rho))
+    dt = 1 / 400 / tscale
+    coll = dict(d=0.12, h=0.2, r=0.025, theta_t=5 * math.pi / 180, lambda_max=100 * tscale, epsilon=0.8)
+    Gd = (0.05 * np.eye(2)) @ (0.05 * np.eye(2)).T
+    b = np.array([0.2, 0.2]) * tscale
+    Ht = np.eye(2) * tscale ** 1.5
+    G = 0.5 * Ht @ Ht.T
+    R = rotation_grid(B)
+    mR = np.stack([R[..., 2, 1], -R[..., 2, 0]])                      # [R32; -R31] (pendulum_reduced_hybrid.m:118)
+    th = -2 * math.pi / 3
+    U = np.array([[math.cos(th), 0, math.sin(th)], [0, 1, 0], [-math.sin(th), 0, math.cos(th)]])
+    Sigma = (2 * tscale) ** 2 * np.eye(2)
+    out = {}
+    for name, prec in (('mixed', hp.HP_MIXED), ('fp64', hp.HP_FP64)):
+        plan = hp.Plan(B, Bx, 2, prec, hp.HP_REAL)
+        plan.set_den_model(L, b, G, mR)
+        t0 = time.perf_counter()
+        c = hp.Collision(plan, L=L, Gd=Gd, nD=10, **coll)
+        torch.cuda.synchronize(dev)
+        t_tables = time.perf_counter() - t0
+        st = hp.State(plan)
+        st.init_mf_gauss(U, (15.0, 15.0, 15.0), np.eye(3), np.zeros(2), Sigma)
+        for _ in range(args.warmup):
+            st.hybrid_step(c, dt, 'euler', 1)
+            st.moments()
+        torch.cuda.synchronize(dev)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        for _ in range(args.steps):
+            st.hybrid_step(c, dt, 'euler', 1)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        tm = time.perf_counter()
+        for _ in range(args.steps):
+            st.moments()
+        t_mom = (time.perf_counter() - tm) / args.steps
+        ms = e0.elapsed_time(e1) / args.steps
+        plan.profile(True)
+        for _ in range(2):
+            st.hybrid_step(c, dt, 'euler', 1)
+        torch.cuda.synchronize(dev)
+        fam = {k: round(v[0] / 2, 3) for k, v in plan.profile_read().items()}
+        plan.profile(False)
+        mo = st.moments()
+        out[name] = {'ms_per_step': round(ms, 3), 'steps_per_s': round(1000.0 / (ms + 1000 * t_mom), 3),
+                     'moments_ms': round(1000 * t_mom, 3), 'colliding_attitudes': c.numR,
+                     'tables_s': round(t_tables, 2), 'mass': mo['mass'], 'ER': mo['ER'].tolist(),
+                     'kernel_ms_per_step': fam}
+        del st, c, plan
+        torch.cuda.empty_cache()
+    er = np.array(out['mixed']['ER']) - np.array(out['fp64']['ER'])
+    line = {'metric': 'hybrid FP steps/s, pendulum_reduced_hybrid sizes (B=30, omega 60x60)',
+            'value': out['mixed']['steps_per_s'], 'unit': 'steps/s', 'higher_is_better': True, 'n_gpus': 1,
+            'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32 (f64 accumulation)', 'data': 'synthetic',
+            'config': {'workload': 'hybrid loop body incl. get_stat moments', 'B': B, 'omega_grid': '60x60',
+                       'dt': dt, 'method': 'euler'},
+            'mixed': out['mixed'], 'fp64': out['fp64'],
+            'ER_max_abs_diff_mixed_vs_fp64': float(np.abs(er).max())}
+    for k in ('mixed', 'fp64'):
+        line[k].pop('ER')
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

@@ -511,6 +511,33 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr int P = pick_p();
 };
 
+// (m, n) pairs with their row start, l-run length, m slot and n bin, longest
+// runs first (the order keeps the lanes of a warp on loops of similar length)
+template <int B, bool CPLX>
+static int build_pairs(hp_plan* p, int2* dpairs) {
+  constexpr int NB2 = 2 * B, NM = CPLX ? 2 * B - 1 : B, NPAIR = NM * (2 * B - 1);
+  std::vector<std::pair<int, int2>> v;
+  const int lmax = B - 1, D = 2 * lmax + 1, mlo = CPLX ? -lmax : 0;
+  for (int mi = 0; mi < NM; ++mi)
+    for (int n = -lmax; n <= lmax; ++n) {
+      const int m = mi + mlo;
+      const int lmin = std::max(std::abs(m), std::abs(n));
+      const int len = lmax - lmin + 1;
+      const int q = n >= 0 ? n : n + NB2;
+      int2 e;
+      e.x = p->h_seg[(size_t)(m - p->m_lo) * D + n + lmax];
+      e.y = len | (mi << 8) | (q << 16) | ((n == 0 ? 1 : 0) << 24);
+      v.push_back({len, e});
+    }
+  std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int2>& a, const std::pair<int, int2>& b) {
+    return a.first > b.first;
+  });
+  std::vector<int2> h;
+  for (auto& x : v) h.push_back(x.second);
+  HP_CUDA_TRY(cudaMemcpy(dpairs, h.data(), sizeof(int2) * NPAIR, cudaMemcpyHostToDevice));
+  return HP_OK;
+}
+
 template <typename T>
 __global__ void k_sd_table(RowLayout L, const T* __restrict__ wig, T* __restrict__ out, int NB, int ngroups,
                            int synth, const double* __restrict__ qw = nullptr) {
@@ -557,27 +584,8 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   int2* dpairs = (int2*)p->ws_get(key, sizeof(int2) * NPAIR, &st);
   if (st) return st;
   if (!have) {
-    // (m, n) pairs with their row start, l-run length, m slot and n bin,
-    // longest runs first
-    std::vector<std::pair<int, int2>> v;
-    const int lmax = B - 1, D = 2 * lmax + 1, mlo = CPLX ? -lmax : 0;
-    for (int mi = 0; mi < NM; ++mi)
-      for (int n = -lmax; n <= lmax; ++n) {
-        const int m = mi + mlo;
-        const int lmin = std::max(std::abs(m), std::abs(n));
-        const int len = lmax - lmin + 1;
-        const int q = n >= 0 ? n : n + NB2;
-        int2 e;
-        e.x = p->h_seg[(size_t)(m - p->m_lo) * D + n + lmax];
-        e.y = len | (mi << 8) | (q << 16) | ((n == 0 ? 1 : 0) << 24);
-        v.push_back({len, e});
-      }
-    std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int2>& a, const std::pair<int, int2>& b) {
-      return a.first > b.first;
-    });
-    std::vector<int2> h;
-    for (auto& x : v) h.push_back(x.second);
-    HP_CUDA_TRY(cudaMemcpy(dpairs, h.data(), sizeof(int2) * NPAIR, cudaMemcpyHostToDevice));
+    st = build_pairs<B, CPLX>(p, dpairs);
+    if (st) return st;
   }
   const int ngroups = (NB2 + NB - 1) / NB;
   const T* dtab = sizeof(T) == 8 ? (const T*)(const void*)p->wig64 : (const T*)(const void*)p->wig32;
@@ -695,6 +703,206 @@ static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out,
 }
 
 // Forward transform of (mult .) f into [row][omega] coefficients of type c2<T>.
+// ----------------------------------------- analysis without atomics ----
+// Stage 1 (k_anal_ag): block = (beta, chunk of PA omega points).  For each
+// omega point the alpha FFT over a and the gamma FFT over c of f(., b, ., w)
+// (times an optional grid multiplier) give Q_b[m][n]; it is written to
+// Qg[(m, n bin)][b][w] with the chunk's omega points consecutive.
+// Stage 2 (k_anal_beta): thread = ((m, n) pair, omega point), all l of the
+// pair: F^l_mn[w] = sum_b w_b d^l_mn(beta_b) Q_b[m][n][w], written straight
+// into the [row][omega] layout.  Every output has one owner: no atomics.
+template <int B, typename T, int PA, bool CPLX>
+__global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, const double* __restrict__ mult,
+                                                 c2<T>* __restrict__ Qg, long long w0, long long nwc) {
+  using C = c2<T>;
+  constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
+  constexpr int NM = CPLX ? D : B;
+  constexpr int MLO = CPLX ? -lmax : 0;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sIn = reinterpret_cast<C*>(smraw);                                   // [PA][c][a]
+  C* sQ = sIn + PA * NB2 * NB2;                                           // [PA][m][c or q]
+  const int b = blockIdx.y;
+  const long long wl0 = (long long)blockIdx.x * PA;                       // chunk-local omega
+  const int pc = (int)min((long long)PA, nwc - wl0);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int NG = NB2 * NB2;
+  // load f(a, b, c, w) for this beta: runs of 2B consecutive a
+  for (int e = tid; e < pc * NG; e += nth) {
+    const int pp = e / NG, r = e % NG, cc = r / NB2, a = r % NB2;
+    const long long w = w0 + wl0 + pp;
+    const long long gi = (long long)a + NB2 * ((long long)b + NB2 * ((long long)cc + NB2 * w));
+    C v;
+    if (CPLX) v = reinterpret_cast<const C*>(fin)[gi];
+    else { v.x = reinterpret_cast<const T*>(fin)[gi]; v.y = 0; }
+    if (mult) {
+      const T mv = (T)mult[a + NB2 * (b + NB2 * cc)];
+      v.x *= mv;
+      v.y *= mv;
+    }
+    sIn[e] = v;
+  }
+  __syncthreads();
+  // alpha: item (p, c): FFT(+) over a, keep the stored m bins
+  for (int it = tid; it < pc * NB2; it += nth) {
+    const int pp = it / NB2, cc = it % NB2;
+    const C* src = sIn + (size_t)it * NB2;
+    C x[NB2];
+#pragma unroll
+    for (int a = 0; a < NB2; ++a) x[a] = src[a];
+    fft<NB2, true>(x);
+    C* dst = sQ + (size_t)pp * NM * NB2 + cc;
+#pragma unroll
+    for (int mi = 0; mi < NM; ++mi) {
+      const int m = mi + MLO;
+      dst[(size_t)mi * NB2] = x[m >= 0 ? m : m + NB2];
+    }
+  }
+  __syncthreads();
+  // gamma: item (p, m): FFT(+) over c, in place (bins n mod 2B)
+  for (int it = tid; it < pc * NM; it += nth) {
+    C* row = sQ + (size_t)it * NB2;
+    C x[NB2];
+#pragma unroll
+    for (int j = 0; j < NB2; ++j) x[j] = row[j];
+    fft<NB2, true>(x);
+#pragma unroll
+    for (int j = 0; j < NB2; ++j) row[j] = x[j];
+  }
+  __syncthreads();
+  // store: Qg[((m * 2B + q) * 2B + b) * nwc + w], consecutive omega points
+  for (int e = tid; e < NM * NB2 * pc; e += nth) {
+    const int pp = e % pc, mq = e / pc;
+    Qg[((long long)mq * NB2 + b) * nwc + wl0 + pp] = sQ[(size_t)pp * NM * NB2 + mq];
+  }
+}
+
+template <int B, typename T, bool CPLX>
+__global__ void __launch_bounds__(256) k_anal_beta(RowLayout L, const c2<T>* __restrict__ Qg,
+                                                   const T* __restrict__ dw, const int2* __restrict__ pairs,
+                                                   int npairs, c2<T>* __restrict__ out, long long w0, long long nwc) {
+  using C = c2<T>;
+  constexpr int NB2 = 2 * B;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pi = blockIdx.y * (blockDim.x >> 5) + warp;
+  if (pi >= npairs) return;
+  const long long wl = (long long)blockIdx.x * 32 + lane;
+  if (wl >= nwc) return;
+  const int2 pe = pairs[pi];
+  const int s = pe.x, len = pe.y & 0xff, mi = (pe.y >> 8) & 0xff, q = (pe.y >> 16) & 0xff;
+  const C* qsrc = Qg + ((long long)(mi * NB2 + q) * NB2) * nwc + wl;
+  const T* dsrc = dw + (size_t)s * NB2;
+  C acc[B];
+#pragma unroll
+  for (int j = 0; j < B; ++j) acc[j] = czero<C>();
+  for (int b0 = 0; b0 < NB2; b0 += 4) {
+    C v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = (b0 + u < NB2) ? qsrc[(long long)(b0 + u) * nwc] : czero<C>();
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      if (j < len) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (b0 + u < NB2) {
+            const T d = __ldg(dsrc + (size_t)j * NB2 + b0 + u);
+            acc[j].x = fma(d, v[u].x, acc[j].x);
+            acc[j].y = fma(d, v[u].y, acc[j].y);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < B; ++j)
+    if (j < len) out[(long long)(s + j) * L.nx + w0 + wl] = acc[j];
+}
+
+// dw[row][b] = w_b d^l_mn(beta_b)
+template <typename T>
+__global__ void k_dw_table(RowLayout L, const T* __restrict__ wig, const double* __restrict__ qw,
+                           T* __restrict__ dw) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int NB2 = 2 * L.B;
+  if (t >= L.nrows * NB2) return;
+  const long long r = t / NB2;
+  const int b = (int)(t % NB2);
+  dw[t] = (T)(qw[b] * (double)wig[(size_t)b * L.nrows + r]);
+}
+
+// largest omega batch (16, 8, 4, 2, 1) whose stage-1 tiles fit 110 KB
+template <int B, typename T, bool CPLX> struct AnalCfg {
+  static constexpr int NM = CPLX ? 2 * B - 1 : B;
+  static constexpr long long bytes(int pa) { return (long long)pa * (2 * B) * (2 * B + NM) * 2 * (long long)sizeof(T); }
+  static constexpr int pick() {
+    int pa = 16;
+    while (pa > 1 && bytes(pa) > 110 * 1024) pa /= 2;
+    return pa;
+  }
+  static constexpr int PA = pick();
+};
+
+template <int B, typename T, bool CPLX>
+static int anal2_launch(hp_plan* p, const void* f, const double* mult, c2<T>* out, cudaStream_t s) {
+  using C = c2<T>;
+  using Cfg = AnalCfg<B, T, CPLX>;
+  constexpr int PA = Cfg::PA, NB2 = 2 * B, NM = Cfg::NM;
+  const size_t smem = (size_t)Cfg::bytes(PA);
+  if (smem > (size_t)smem_limit()) { hp_set_error("analysis tiles exceed shared memory"); return HP_ERR_UNSUPPORTED; }
+  int st = HP_OK;
+  // pair table (shared with the synthesis) and the w_b d table
+  constexpr int NPAIR = NM * (2 * B - 1);
+  const char* key = CPLX ? "tf.pairs_c" : "tf.pairs_r";
+  bool have = false;
+  for (auto& kv : p->ws) if (kv.first == key) have = true;
+  int2* dpairs = (int2*)p->ws_get(key, sizeof(int2) * NPAIR, &st);
+  if (st) return st;
+  if (!have) {
+    st = build_pairs<B, CPLX>(p, dpairs);
+    if (st) return st;
+  }
+  const char* dkey = sizeof(T) == 8 ? "tf.dw64" : "tf.dw32";
+  have = false;
+  for (auto& kv : p->ws) if (kv.first == dkey) have = true;
+  T* dw = (T*)p->ws_get(dkey, sizeof(T) * p->nrows * NB2, &st);
+  if (st) return st;
+  if (!have) {
+    const long long n = p->nrows * NB2;
+    k_dw_table<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+        p->layout(), sizeof(T) == 8 ? (const T*)(const void*)p->wig64 : (const T*)(const void*)p->wig32, p->qw, dw);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  // omega chunks keep the staged tiles within 2 GB
+  const long long per_w = (long long)NM * NB2 * NB2 * (long long)sizeof(C);
+  long long nwc = std::max(32LL, (2LL << 30) / per_w / 32 * 32);
+  nwc = std::min(nwc, (p->nx + 31) / 32 * 32);
+  C* Qg = (C*)p->ws_get("tf.Q", (size_t)per_w * nwc, &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_anal_ag<B, T, PA, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ProfScope _ps(p, "tf.anal", s);
+  for (long long w0 = 0; w0 < p->nx; w0 += nwc) {
+    const long long nw = std::min(nwc, p->nx - w0);
+    dim3 ga((unsigned)((nw + PA - 1) / PA), (unsigned)NB2);
+    k_anal_ag<B, T, PA, CPLX><<<ga, 256, smem, s>>>(f, mult, Qg, w0, nw);
+    HP_CUDA_TRY(cudaGetLastError());
+    dim3 gb((unsigned)((nw + 31) / 32), (unsigned)((NPAIR + 7) / 8));
+    k_anal_beta<B, T, CPLX><<<gb, 256, 0, s>>>(p->layout(), Qg, dw, dpairs, NPAIR, out, w0, nw);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  return HP_OK;
+}
+
+template <typename T, bool CPLX>
+static int anal2_any(hp_plan* p, const void* f, const double* mult, c2<T>* out, cudaStream_t s) {
+  switch (p->B) {
+#define X(b) case b: return anal2_launch<b, T, CPLX>(p, f, mult, out, s);
+    HP_FOR_EACH_B(X)
+#undef X
+    default:
+      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
 template <typename T>
 static int forward_rows_T(hp_plan* p, const void* f, int complex_in, const double* mult, c2<T>* out,
                           cudaStream_t s) {
@@ -705,12 +913,9 @@ static int forward_rows_T(hp_plan* p, const void* f, int complex_in, const doubl
   if (st) return st;
   C* t2 = (C*)p->ws_get("tf.t2", fb, &st);
   if (st) return st;
-  st = complex_in ? anal_any<T, true>(p, f, mult, t1, s) : anal_any<T, false>(p, f, mult, t1, s);
+  (void)t1;
+  st = complex_in ? anal2_any<T, true>(p, f, mult, t2, s) : anal2_any<T, false>(p, f, mult, t2, s);
   if (st) return st;
-  dim3 grid((unsigned)((p->nrows + 31) / 32), (unsigned)((p->nx + 31) / 32));
-  { ProfScope _ps(p, "tf.transpose", s);
-  k_transpose<T, T><<<grid, dim3(32, 8), 0, s>>>(t1, t2, p->nx, p->nrows); }
-  HP_CUDA_TRY(cudaGetLastError());
   return omega_fft_any<T, T>(p, t2, out, false, s);
 }
 
