@@ -87,23 +87,6 @@ __global__ void __launch_bounds__(128) k_wline(const c2<T>* __restrict__ in, c2<
   for (int j = 0; j < N; ++j) dst[j * plane] = scale * x[j];
 }
 
-// out[c][r] = in[r][c] for an R x Cc matrix of complex T (32x32 tiles).
-template <typename Tin, typename Tout>
-__global__ void k_transpose(const c2<Tin>* __restrict__ in, c2<Tout>* __restrict__ out, long long R,
-                            long long Cc) {
-  __shared__ c2<Tout> tile[32][33];
-  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const long long r = r0 + k, c = c0 + threadIdx.x;
-    if (r < R && c < Cc) tile[k][threadIdx.x] = cvt<c2<Tout>, c2<Tin>>(in[r * Cc + c]);
-  }
-  __syncthreads();
-  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
-    const long long c = c0 + k, r = r0 + threadIdx.x;
-    if (r < R && c < Cc) out[c * R + r] = tile[threadIdx.x][k];
-  }
-}
-
 template <typename T>
 __global__ void k_to_c64(const c2<T>* __restrict__ in, double2* __restrict__ out, long long n) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -305,116 +288,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   }
 }
 
-// ------------------------------------------------------------- analysis ----
-// Block = (group of NB betas, range of omega points).  Per omega point:
-//   alpha stage  Q1[c][m] = sum_a f[a][b][c] e^{+i m alpha_a}
-//   gamma stage  Q[m][n]  = sum_c Q1[c][m] e^{+i n gamma_c}
-//   beta  stage  Fa[w][(m,n,l)] += sum_b w_b d^l_mn(beta_b) Q_b[m][n]
-// The beta sum over groups of betas is accumulated with atomics.
-// GD: w_b d of the block's betas from a global table [group][NB][row]
-// (large bandlimits) instead of staging it from the d table `wig`.
-template <int B, typename T, int NB, bool CPLX, bool GD>
-__global__ void __launch_bounds__(512) k_anal(RowLayout L, const void* __restrict__ fin,
-                                              const T* __restrict__ wig, const double* __restrict__ qw,
-                                              const double* __restrict__ mult,
-                                              c2<T>* __restrict__ Fa, int P, long long w_per_block) {
-  using C = c2<T>;
-  constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
-  constexpr int NM = CPLX ? D : B;
-  constexpr int MLO = CPLX ? -lmax : 0;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sds = reinterpret_cast<T*>(smraw);  // [NB][nrows] w_b d
-  const T* sd = GD ? wig + (size_t)blockIdx.y * NB * L.nrows : sds;
-  size_t off = GD ? 0 : ((size_t)NB * L.nrows * sizeof(T) + 15) / 16 * 16;
-  C* sQ = reinterpret_cast<C*>(smraw + off);  // [P][NB][NM][NB2] (n bins)
-  size_t off2 = off + (size_t)P * NB * NM * NB2 * sizeof(C);
-  C* sIn = reinterpret_cast<C*>(smraw + off2);  // [P][NB][NB2 (c)][NB2 (a)]
-  const int b0 = blockIdx.y * NB;
-  const int nbv = min(NB, NB2 - b0);
-  const int tid = threadIdx.x, nth = blockDim.x;
-  for (long long e = tid; !GD && e < (long long)NB * L.nrows; e += nth) {
-    const int bb = (int)(e / L.nrows);
-    sds[e] = (bb < nbv) ? (T)(qw[b0 + bb] * (double)wig[(long long)(b0 + bb) * L.nrows + e % L.nrows]) : (T)0;
-  }
-  const long long wbeg = blockIdx.x * w_per_block;
-  const long long wend = min(wbeg + w_per_block, L.nx);
-  for (long long w0 = wbeg; w0 < wend; w0 += P) {
-    const int pc = (int)min((long long)P, wend - w0);
-    __syncthreads();
-    // load f lines into sIn[p][bb][c][a]
-    const long long per_w = (long long)NB2 * nbv * NB2;
-    for (long long e = tid; e < (long long)pc * per_w; e += nth) {
-      const int pp = (int)(e / per_w), r = (int)(e % per_w);
-      const int cc = r / (nbv * NB2), bq = (r / NB2) % nbv, a = r % NB2;
-      const long long gi = (long long)a + NB2 * ((long long)(b0 + bq) + NB2 * ((long long)cc + NB2 * (w0 + pp)));
-      C v;
-      if (CPLX) v = reinterpret_cast<const C*>(fin)[gi];
-      else { v.x = reinterpret_cast<const T*>(fin)[gi]; v.y = 0; }
-      if (mult) {  // pointwise multiplier on the rotation grid (index a + 2B b + 4B^2 c)
-        const T mv = (T)mult[a + NB2 * ((b0 + bq) + NB2 * cc)];
-        v.x *= mv;
-        v.y *= mv;
-      }
-      sIn[(((size_t)pp * NB + bq) * NB2 + cc) * NB2 + a] = v;
-    }
-    __syncthreads();
-    // alpha stage: item (p, bb, c): FFT(+) over a, keep stored m bins -> sQ[p][bb][mi][c]
-    for (int it = tid; it < pc * nbv * NB2; it += nth) {
-      const int pp = it / (nbv * NB2), bq = (it / NB2) % nbv, cc = it % NB2;
-      const C* src = sIn + (((size_t)pp * NB + bq) * NB2 + cc) * NB2;
-      C x[NB2];
-#pragma unroll
-      for (int a = 0; a < NB2; ++a) x[a] = src[a];
-      fft<NB2, true>(x);
-      C* dst = sQ + ((size_t)(pp * NB + bq) * NM) * NB2 + cc;
-#pragma unroll
-      for (int mi = 0; mi < NM; ++mi) {
-        const int m = mi + MLO;
-        dst[(size_t)mi * NB2] = x[m >= 0 ? m : m + NB2];
-      }
-    }
-    __syncthreads();
-    // gamma stage: item (p, bb, mi): FFT(+) over c, in place (bins n mod 2B)
-    for (int it = tid; it < pc * nbv * NM; it += nth) {
-      const int pp = it / (nbv * NM), bq = (it / NM) % nbv, mi = it % NM;
-      C* row = sQ + ((size_t)(pp * NB + bq) * NM + mi) * NB2;
-      C x[NB2];
-#pragma unroll
-      for (int j = 0; j < NB2; ++j) x[j] = row[j];
-      fft<NB2, true>(x);
-#pragma unroll
-      for (int j = 0; j < NB2; ++j) row[j] = x[j];
-    }
-    __syncthreads();
-    // beta stage: item (p, m, n): sum over the group's betas, atomically added
-    const int npairs = NM * D;
-    for (int it = tid; it < pc * npairs; it += nth) {
-      const int pp = it / npairs, pr = it % npairs;
-      const int mi = pr / D, n = pr % D - lmax, m = mi + MLO;
-      const int am = abs(m), an = abs(n), lmin = am > an ? am : an;
-      if (lmin > lmax) continue;
-      const int q = n >= 0 ? n : n + NB2;
-      const long long s = L.seg[(m - L.m_lo) * D + n + lmax];
-      C* dst = Fa + (w0 + pp) * L.nrows + s;
-      for (int j = 0; j <= lmax - lmin; ++j) {
-        C acc = czero<C>();
-        for (int bq = 0; bq < nbv; ++bq) {
-          const T dv = sd[(size_t)bq * L.nrows + s + j];
-          const C v = sQ[((size_t)(pp * NB + bq) * NM + mi) * NB2 + q];
-          acc.x += dv * v.x;
-          acc.y += dv * v.y;
-        }
-        atomicAdd(&dst[j].x, acc.x);
-        atomicAdd(&dst[j].y, acc.y);
-      }
-    }
-  }
-}
-
 // -------------------------------------------------------------- drivers ----
-template <typename T> struct TfCfg;
-template <> struct TfCfg<double> { static constexpr int NB = 2; static constexpr int threads = 256; };
-template <> struct TfCfg<float> { static constexpr int NB = 4; static constexpr int threads = 512; };
 
 static int smem_limit() {
   int dev = 0, v = 0;
@@ -615,53 +489,6 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   return HP_OK;
 }
 
-template <int B, typename T, bool CPLX>
-static int anal_launch(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
-  using C = c2<T>;
-  // fewer betas per block at the largest bandlimit (the per-omega tiles grow as B^2)
-  constexpr int NB = B >= 24 ? (sizeof(T) == 8 ? 1 : 2) : TfCfg<T>::NB, NB2 = 2 * B;
-  constexpr int NM = CPLX ? 2 * B - 1 : B;
-  constexpr long long NROWS = CPLX ? (long long)B * (2 * B - 1) * (2 * B + 1) / 3 : (long long)B * (B + 1) * (4 * B - 1) / 6;
-  constexpr bool GD = NB * NROWS * (long long)sizeof(T) > 64 * 1024;
-  const int threads = TfCfg<T>::threads;
-  const size_t sd_bytes = GD ? 0 : ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
-  const size_t per_p = (size_t)NB * NM * NB2 * sizeof(C) + (size_t)NB * NB2 * NB2 * sizeof(C);
-  const int lim = smem_limit();
-  int P = 4;
-  while (P > 1 && sd_bytes + P * per_p > (size_t)lim) --P;
-  if (sd_bytes + P * per_p > (size_t)lim) {
-    hp_set_error("analysis tables exceed shared memory for this bandlimit");
-    return HP_ERR_UNSUPPORTED;
-  }
-  const size_t smem = sd_bytes + P * per_p;
-  const int ngroups = (NB2 + NB - 1) / NB;
-  const T* dtab = sizeof(T) == 8 ? (const T*)(const void*)p->wig64 : (const T*)(const void*)p->wig32;
-  if (GD) {   // w_b d as [group][NB][row], built once per plan
-    int st = HP_OK;
-    const char* gkey = sizeof(T) == 8 ? (CPLX ? "tf.sda64c" : "tf.sda64") : (CPLX ? "tf.sda32c" : "tf.sda32");
-    bool hv = false;
-    for (auto& kv : p->ws) if (kv.first == gkey) hv = true;
-    const long long n = (long long)ngroups * p->nrows * NB;
-    T* sdg = (T*)p->ws_get(gkey, sizeof(T) * n, &st);
-    if (st) return st;
-    if (!hv) {
-      k_sd_table<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), dtab, sdg, NB, ngroups, 0, p->qw);
-      HP_CUDA_TRY(cudaGetLastError());
-    }
-    dtab = sdg;
-  }
-  long long wblocks = std::max(1LL, std::min(p->nx, 8LL * 148 * 2 / ngroups + 1));
-  long long wpb = (p->nx + wblocks - 1) / wblocks;
-  wpb = (wpb + P - 1) / P * P;
-  wblocks = (p->nx + wpb - 1) / wpb;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_anal<B, T, NB, CPLX, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid((unsigned)wblocks, (unsigned)ngroups);
-  HP_CUDA_TRY(cudaMemsetAsync(Fa, 0, sizeof(C) * p->nrows * p->nx, s));
-  ProfScope _ps(p, "tf.anal", s);
-  k_anal<B, T, NB, CPLX, GD><<<grid, threads, smem, s>>>(p->layout(), f, dtab, p->qw, mult, Fa, P, wpb);
-  HP_CUDA_TRY(cudaGetLastError());
-  return HP_OK;
-}
 
 #define HP_FOR_EACH_B(X) X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(24) X(30) X(32)
 
@@ -677,17 +504,6 @@ static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   }
 }
 
-template <typename T, bool CPLX>
-static int anal_any(hp_plan* p, const void* f, const double* mult, c2<T>* Fa, cudaStream_t s) {
-  switch (p->B) {
-#define X(b) case b: return anal_launch<b, T, CPLX>(p, f, mult, Fa, s);
-    HP_FOR_EACH_B(X)
-#undef X
-    default:
-      hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)");
-      return HP_ERR_UNSUPPORTED;
-  }
-}
 
 template <typename T>
 static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s) {
@@ -719,8 +535,10 @@ __global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, c
   constexpr int NM = CPLX ? D : B;
   constexpr int MLO = CPLX ? -lmax : 0;
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* sIn = reinterpret_cast<C*>(smraw);                                   // [PA][c][a]
-  C* sQ = sIn + PA * NB2 * NB2;                                           // [PA][m][c or q]
+  // input tile [PA][c][a]: complex, or real values for real densities
+  C* sIn = reinterpret_cast<C*>(smraw);
+  T* sInR = reinterpret_cast<T*>(smraw);
+  C* sQ = reinterpret_cast<C*>(smraw + (size_t)PA * NB2 * NB2 * (CPLX ? sizeof(C) : sizeof(T)));   // [PA][m][c or q]
   const int b = blockIdx.y;
   const long long wl0 = (long long)blockIdx.x * PA;                       // chunk-local omega
   const int pc = (int)min((long long)PA, nwc - wl0);
@@ -731,19 +549,43 @@ __global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, c
     const int pp = e / NG, r = e % NG, cc = r / NB2, a = r % NB2;
     const long long w = w0 + wl0 + pp;
     const long long gi = (long long)a + NB2 * ((long long)b + NB2 * ((long long)cc + NB2 * w));
-    C v;
-    if (CPLX) v = reinterpret_cast<const C*>(fin)[gi];
-    else { v.x = reinterpret_cast<const T*>(fin)[gi]; v.y = 0; }
-    if (mult) {
-      const T mv = (T)mult[a + NB2 * (b + NB2 * cc)];
+    const T mv = mult ? (T)mult[a + NB2 * (b + NB2 * cc)] : (T)1;
+    if (CPLX) {
+      C v = reinterpret_cast<const C*>(fin)[gi];
       v.x *= mv;
       v.y *= mv;
+      sIn[e] = v;
+    } else {
+      sInR[e] = reinterpret_cast<const T*>(fin)[gi] * mv;
     }
-    sIn[e] = v;
   }
   __syncthreads();
-  // alpha: item (p, c): FFT(+) over a, keep the stored m bins
-  for (int it = tid; it < pc * NB2; it += nth) {
+  // alpha, real densities: item (p, c pair): columns c, c+1 share one complex
+  // FFT, z = f_c + i f_{c+1}: X_c[m] = (Z[m] + conj Z[-m]) / 2,
+  // X_{c+1}[m] = (Z[m] - conj Z[-m]) / 2i
+  for (int it = tid; !CPLX && it < pc * B; it += nth) {
+    const int pp = it / B, c0 = 2 * (it % B);
+    const T* r0 = sInR + ((size_t)pp * NB2 + c0) * NB2;
+    const T* r1 = r0 + NB2;
+    C x[NB2];
+#pragma unroll
+    for (int a = 0; a < NB2; ++a) { x[a].x = r0[a]; x[a].y = r1[a]; }
+    fft<NB2, true>(x);
+    C* dst = sQ + (size_t)pp * NM * NB2 + c0;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+      const C zp = x[m], zm = x[(NB2 - m) % NB2];
+      C u, v;
+      u.x = (T)0.5 * (zp.x + zm.x);
+      u.y = (T)0.5 * (zp.y - zm.y);
+      v.x = (T)0.5 * (zp.y + zm.y);
+      v.y = (T)0.5 * (zm.x - zp.x);
+      dst[(size_t)m * NB2] = u;
+      dst[(size_t)m * NB2 + 1] = v;
+    }
+  }
+  // alpha, complex densities: item (p, c): FFT(+) over a, keep the stored m bins
+  for (int it = tid; CPLX && it < pc * NB2; it += nth) {
     const int pp = it / NB2, cc = it % NB2;
     const C* src = sIn + (size_t)it * NB2;
     C x[NB2];
@@ -829,13 +671,17 @@ __global__ void k_dw_table(RowLayout L, const T* __restrict__ wig, const double*
   dw[t] = (T)(qw[b] * (double)wig[(size_t)b * L.nrows + r]);
 }
 
-// largest omega batch (16, 8, 4, 2, 1) whose stage-1 tiles fit 110 KB
+// largest omega batch (16, 8, 4, 2, 1) whose stage-1 tiles fit the budget
 template <int B, typename T, bool CPLX> struct AnalCfg {
   static constexpr int NM = CPLX ? 2 * B - 1 : B;
-  static constexpr long long bytes(int pa) { return (long long)pa * (2 * B) * (2 * B + NM) * 2 * (long long)sizeof(T); }
+  static constexpr long long bytes(int pa) {
+    return (long long)pa * (2 * B) * ((2 * B) * (CPLX ? 2 : 1) + 2 * NM) * (long long)sizeof(T);
+  }
+  // two resident blocks where a batch of 4 fits 110 KB, else one block of up to 220 KB
+  static constexpr long long cap() { return bytes(4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
   static constexpr int pick() {
     int pa = 16;
-    while (pa > 1 && bytes(pa) > 110 * 1024) pa /= 2;
+    while (pa > 1 && bytes(pa) > cap()) pa /= 2;
     return pa;
   }
   static constexpr int PA = pick();
@@ -878,12 +724,15 @@ static int anal2_launch(hp_plan* p, const void* f, const double* mult, c2<T>* ou
   C* Qg = (C*)p->ws_get("tf.Q", (size_t)per_w * nwc, &st);
   if (st) return st;
   HP_CUDA_TRY(cudaFuncSetAttribute(k_anal_ag<B, T, PA, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  ProfScope _ps(p, "tf.anal", s);
   for (long long w0 = 0; w0 < p->nx; w0 += nwc) {
     const long long nw = std::min(nwc, p->nx - w0);
-    dim3 ga((unsigned)((nw + PA - 1) / PA), (unsigned)NB2);
-    k_anal_ag<B, T, PA, CPLX><<<ga, 256, smem, s>>>(f, mult, Qg, w0, nw);
-    HP_CUDA_TRY(cudaGetLastError());
+    {
+      ProfScope _ps(p, "tf.anal.ag", s);
+      dim3 ga((unsigned)((nw + PA - 1) / PA), (unsigned)NB2);
+      k_anal_ag<B, T, PA, CPLX><<<ga, 256, smem, s>>>(f, mult, Qg, w0, nw);
+      HP_CUDA_TRY(cudaGetLastError());
+    }
+    ProfScope _ps(p, "tf.anal.beta", s);
     dim3 gb((unsigned)((nw + 31) / 32), (unsigned)((NPAIR + 7) / 8));
     k_anal_beta<B, T, CPLX><<<gb, 256, 0, s>>>(p->layout(), Qg, dw, dpairs, NPAIR, out, w0, nw);
     HP_CUDA_TRY(cudaGetLastError());
