@@ -158,36 +158,19 @@ __global__ void k_coll_df(int nx, int nR, int numR, int nD, const int* __restric
 }
 
 // f += dt * df(f) in place (pendulum_reduced_hybrid.m:232-233): the colliding
-// columns are first gathered into fk[ix][k] so that every tap reads the
-// pre-update density.
-template <typename T>
-__global__ void k_coll_gather(int nx, int nR, int numR, const int* __restrict__ indR, const T* __restrict__ f,
-                              T* __restrict__ fk) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)nx * numR) return;
-  const int k = (int)(t % numR), ix = (int)(t / numR);
-  fk[t] = f[(long long)ix * nR + indR[k]];
-}
-
-template <typename T>
-__global__ void k_coll_update(int nx, int nR, int numR, int nD, const int* __restrict__ indR,
-                              const double* __restrict__ lambda, const double* __restrict__ fcL,
-                              const short* __restrict__ idx, const T* __restrict__ fk, T* __restrict__ f,
-                              double dt) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)nx * numR) return;
-  const int k = (int)(t % numR), ix = (int)(t / numR);
-  double s = 0.0;
-  for (int d = 0; d < nD; ++d) s += fcL[t * nD + d] * (double)fk[(long long)idx[t * nD + d] * numR + k];
-  const double f0 = (double)fk[t];
-  f[(long long)ix * nR + indR[k]] = (T)(f0 + dt * (s - lambda[t] * f0));
-}
+// columns are first gathered into fk[k][ix] so that every tap reads the
+// pre-update density (k_coll_gather_t / k_coll_update_t below).
 
 // --------------------------------------------------------------- C ABI ----
 struct hp_collision {
   hp_plan* plan = nullptr;
   CollisionTables t;
   double L = 0;
+  // the tables transposed to [k][d][ix] / [k][ix] in the plan's compute
+  // precision, for the in-place update of the hybrid step (built on first use)
+  void* fcLT = nullptr;
+  short* idxT = nullptr;
+  void* lamT = nullptr;
 };
 
 extern "C" int hp_collision_create(hp_plan* p, const hp_collision_params* prm, hp_collision** out, int* numR) {
@@ -280,6 +263,7 @@ extern "C" int hp_collision_destroy(hp_collision* c) {
   if (!c) return HP_OK;
   cudaFree(c->t.indR); cudaFree(c->t.lambda); cudaFree(c->t.omega); cudaFree(c->t.fcL);
   cudaFree(c->t.idx); cudaFree(c->t.PC);
+  cudaFree(c->fcLT); cudaFree(c->idxT); cudaFree(c->lamT);
   delete c;
   return HP_OK;
 }
@@ -331,18 +315,106 @@ extern "C" int hp_collision_df(hp_collision* c, const double* f, double* df, int
   return HP_OK;
 }
 
+// [ix][k][d] -> [k][d][ix] (and [ix][k] -> [k][ix] for lambda)
+template <typename T>
+__global__ void k_coll_transpose(int nx, int numR, int nD, const double* __restrict__ lambda,
+                                 const double* __restrict__ fcL, const short* __restrict__ idx,
+                                 T* __restrict__ lamT, T* __restrict__ fcLT, short* __restrict__ idxT) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;   // output index, ix fastest
+  const long long n = (long long)nx * numR * (nD + 1);
+  if (t >= n) return;
+  const int ix = (int)(t % nx);
+  const long long r = t / nx;                        // k * (nD + 1) + slot
+  const int k = (int)(r / (nD + 1)), slot = (int)(r % (nD + 1));
+  const long long src = (long long)ix * numR + k;
+  if (slot == nD) {
+    lamT[(long long)k * nx + ix] = (T)lambda[src];
+  } else {
+    fcLT[((long long)k * nD + slot) * nx + ix] = (T)fcL[src * nD + slot];
+    idxT[((long long)k * nD + slot) * nx + ix] = idx[src * nD + slot];
+  }
+}
+
+// fk[k][ix] = f[ix][indR[k]] through a 32 x 32 tile: reads run along k
+// (indR ascending), writes along ix
+template <typename T>
+__global__ void k_coll_gather_t(int nx, long long nR, int numR, const int* __restrict__ indR, const T* __restrict__ f,
+                                T* __restrict__ fk) {
+  __shared__ T tile[32][33];
+  const int k0 = blockIdx.x * 32, x0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int ix = x0 + r, k = k0 + threadIdx.x;
+    tile[r][threadIdx.x] = (ix < nx && k < numR) ? f[(long long)ix * nR + indR[k]] : (T)0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, ix = x0 + threadIdx.x;
+    if (k < numR && ix < nx) fk[(long long)k * nx + ix] = tile[threadIdx.x][r];
+  }
+}
+
+// f[ix][indR[k]] = fk + dt (sum_d fcL fk[k][idx] - lambda fk), computed with ix
+// along lanes (coalesced tables, gathers within one row of fk) and written
+// back through a tile with k along lanes
+template <typename T>
+__global__ void k_coll_update_t(int nx, long long nR, int numR, int nD, const int* __restrict__ indR,
+                                const T* __restrict__ lamT, const T* __restrict__ fcLT,
+                                const short* __restrict__ idxT, const T* __restrict__ fk, T* __restrict__ f,
+                                double dt) {
+  __shared__ T tile[32][33];
+  const int k0 = blockIdx.x * 32, x0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int k = k0 + r, ix = x0 + threadIdx.x;
+    T v = (T)0;
+    if (k < numR && ix < nx) {
+      const T* row = fk + (long long)k * nx;
+      double s = 0.0;
+      for (int d = 0; d < nD; ++d) {
+        const long long o = ((long long)k * nD + d) * nx + ix;
+        s += (double)fcLT[o] * (double)row[idxT[o]];
+      }
+      const double f0 = (double)row[ix];
+      v = (T)(f0 + dt * (s - (double)lamT[(long long)k * nx + ix] * f0));
+    }
+    tile[r][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int ix = x0 + r, k = k0 + threadIdx.x;
+    if (k < numR && ix < nx) f[(long long)ix * nR + indR[k]] = tile[threadIdx.x][r];
+  }
+}
+
 template <typename T>
 static int coll_apply_T(hp_collision* c, T* f, double dt, cudaStream_t s) {
   hp_plan* p = c->plan;
   if (c->t.numR == 0) return HP_OK;
   const long long nR = 8LL * p->B * p->B * p->B, nx = (long long)p->N * p->N, nt = nx * c->t.numR;
+  const int nD = c->t.nD;
   int st = HP_OK;
+  if (!c->fcLT) {
+    if (cudaMalloc(&c->fcLT, sizeof(T) * nt * nD) != cudaSuccess ||
+        cudaMalloc(&c->idxT, sizeof(short) * nt * nD) != cudaSuccess ||
+        cudaMalloc(&c->lamT, sizeof(T) * nt) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(c->fcLT); cudaFree(c->idxT); cudaFree(c->lamT);
+      c->fcLT = c->lamT = nullptr;
+      c->idxT = nullptr;
+      hp_set_error("device allocation failed");
+      return HP_ERR_ALLOC;
+    }
+    const long long n = nt * (nD + 1);
+    k_coll_transpose<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>((int)nx, c->t.numR, nD, c->t.lambda, c->t.fcL,
+                                                                     c->t.idx, (T*)c->lamT, (T*)c->fcLT, c->idxT);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
   T* fk = (T*)p->ws_get("coll.fk", sizeof(T) * nt, &st);
   if (st) return st;
   ProfScope _ps(p, "coll.df", s);
-  k_coll_gather<T><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>((int)nx, (int)nR, c->t.numR, c->t.indR, f, fk);
-  k_coll_update<T><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>((int)nx, (int)nR, c->t.numR, c->t.nD, c->t.indR,
-                                                                c->t.lambda, c->t.fcL, c->t.idx, fk, f, dt);
+  dim3 grid((unsigned)((c->t.numR + 31) / 32), (unsigned)((nx + 31) / 32));
+  k_coll_gather_t<T><<<grid, dim3(32, 8), 0, s>>>((int)nx, nR, c->t.numR, c->t.indR, f, fk);
+  k_coll_update_t<T><<<grid, dim3(32, 8), 0, s>>>((int)nx, nR, c->t.numR, nD, c->t.indR, (const T*)c->lamT,
+                                                   (const T*)c->fcLT, c->idxT, fk, f, dt);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
