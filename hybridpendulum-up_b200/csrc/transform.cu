@@ -535,10 +535,12 @@ __global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, c
   constexpr int NM = CPLX ? D : B;
   constexpr int MLO = CPLX ? -lmax : 0;
   extern __shared__ __align__(16) unsigned char smraw[];
-  // input tile [PA][c][a]: complex, or real values for real densities
+  // input tile [PA][c][a] (complex, or real values for real densities); the
+  // alpha stage reads its lines into registers before a barrier, so its
+  // output [PA][m][c or q] reuses the same shared memory
   C* sIn = reinterpret_cast<C*>(smraw);
   T* sInR = reinterpret_cast<T*>(smraw);
-  C* sQ = reinterpret_cast<C*>(smraw + (size_t)PA * NB2 * NB2 * (CPLX ? sizeof(C) : sizeof(T)));   // [PA][m][c or q]
+  C* sQ = reinterpret_cast<C*>(smraw);
   const int b = blockIdx.y;
   const long long wl0 = (long long)blockIdx.x * PA;                       // chunk-local omega
   const int pc = (int)min((long long)PA, nwc - wl0);
@@ -560,43 +562,51 @@ __global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, c
     }
   }
   __syncthreads();
-  // alpha, real densities: item (p, c pair): columns c, c+1 share one complex
+  // alpha, one item per thread (the host keeps the item count within the
+  // block).  Real densities: item (p, c pair), columns c, c+1 share one complex
   // FFT, z = f_c + i f_{c+1}: X_c[m] = (Z[m] + conj Z[-m]) / 2,
-  // X_{c+1}[m] = (Z[m] - conj Z[-m]) / 2i
-  for (int it = tid; !CPLX && it < pc * B; it += nth) {
-    const int pp = it / B, c0 = 2 * (it % B);
-    const T* r0 = sInR + ((size_t)pp * NB2 + c0) * NB2;
-    const T* r1 = r0 + NB2;
+  // X_{c+1}[m] = (Z[m] - conj Z[-m]) / 2i.  Complex densities: item (p, c).
+  {
+    const int nitems = CPLX ? pc * NB2 : pc * B;
+    const bool act = tid < nitems;
+    const int pp = CPLX ? tid / NB2 : tid / B;
+    const int c0 = CPLX ? tid % NB2 : 2 * (tid % B);
     C x[NB2];
+    if (act) {
+      if (CPLX) {
+        const C* src = sIn + (size_t)tid * NB2;
 #pragma unroll
-    for (int a = 0; a < NB2; ++a) { x[a].x = r0[a]; x[a].y = r1[a]; }
-    fft<NB2, true>(x);
-    C* dst = sQ + (size_t)pp * NM * NB2 + c0;
+        for (int a = 0; a < NB2; ++a) x[a] = src[a];
+      } else {
+        const T* r0 = sInR + ((size_t)pp * NB2 + c0) * NB2;
+        const T* r1 = r0 + NB2;
 #pragma unroll
-    for (int m = 0; m < NM; ++m) {
-      const C zp = x[m], zm = x[(NB2 - m) % NB2];
-      C u, v;
-      u.x = (T)0.5 * (zp.x + zm.x);
-      u.y = (T)0.5 * (zp.y - zm.y);
-      v.x = (T)0.5 * (zp.y + zm.y);
-      v.y = (T)0.5 * (zm.x - zp.x);
-      dst[(size_t)m * NB2] = u;
-      dst[(size_t)m * NB2 + 1] = v;
+        for (int a = 0; a < NB2; ++a) { x[a].x = r0[a]; x[a].y = r1[a]; }
+      }
     }
-  }
-  // alpha, complex densities: item (p, c): FFT(+) over a, keep the stored m bins
-  for (int it = tid; CPLX && it < pc * NB2; it += nth) {
-    const int pp = it / NB2, cc = it % NB2;
-    const C* src = sIn + (size_t)it * NB2;
-    C x[NB2];
+    __syncthreads();
+    if (act) {
+      fft<NB2, true>(x);
+      C* dst = sQ + (size_t)pp * NM * NB2 + c0;
+      if (CPLX) {
 #pragma unroll
-    for (int a = 0; a < NB2; ++a) x[a] = src[a];
-    fft<NB2, true>(x);
-    C* dst = sQ + (size_t)pp * NM * NB2 + cc;
+        for (int mi = 0; mi < NM; ++mi) {
+          const int m = mi + MLO;
+          dst[(size_t)mi * NB2] = x[m >= 0 ? m : m + NB2];
+        }
+      } else {
 #pragma unroll
-    for (int mi = 0; mi < NM; ++mi) {
-      const int m = mi + MLO;
-      dst[(size_t)mi * NB2] = x[m >= 0 ? m : m + NB2];
+        for (int m = 0; m < NM; ++m) {
+          const C zp = x[m], zm = x[(NB2 - m) % NB2];
+          C u, v;
+          u.x = (T)0.5 * (zp.x + zm.x);
+          u.y = (T)0.5 * (zp.y - zm.y);
+          v.x = (T)0.5 * (zp.y + zm.y);
+          v.y = (T)0.5 * (zm.x - zp.x);
+          dst[(size_t)m * NB2] = u;
+          dst[(size_t)m * NB2 + 1] = v;
+        }
+      }
     }
   }
   __syncthreads();
@@ -674,14 +684,18 @@ __global__ void k_dw_table(RowLayout L, const T* __restrict__ wig, const double*
 // largest omega batch (16, 8, 4, 2, 1) whose stage-1 tiles fit the budget
 template <int B, typename T, bool CPLX> struct AnalCfg {
   static constexpr int NM = CPLX ? 2 * B - 1 : B;
-  static constexpr long long bytes(int pa) {
-    return (long long)pa * (2 * B) * ((2 * B) * (CPLX ? 2 : 1) + 2 * NM) * (long long)sizeof(T);
-  }
+  static constexpr long long in_w = (long long)(2 * B) * (2 * B) * (CPLX ? 2 : 1);   // T elements per omega
+  static constexpr long long q_w = 2LL * NM * (2 * B);
+  static constexpr long long bytes(int pa) { return (long long)pa * (in_w > q_w ? in_w : q_w) * (long long)sizeof(T); }
+  static constexpr int items = CPLX ? 2 * B : B;    // alpha items per omega point
+  // threads per block: from B = 24 the 2B-point register FFTs need ~170-255
+  // registers, so two 128-thread blocks per SM overlap loads and FFTs
+  static constexpr int NT = B >= 24 ? 128 : 256;
   // two resident blocks where a batch of 4 fits 110 KB, else one block of up to 220 KB
   static constexpr long long cap() { return bytes(4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
   static constexpr int pick() {
     int pa = 16;
-    while (pa > 1 && bytes(pa) > cap()) pa /= 2;
+    while (pa > 1 && (bytes(pa) > cap() || pa * items > NT)) pa /= 2;
     return pa;
   }
   static constexpr int PA = pick();
@@ -729,7 +743,7 @@ static int anal2_launch(hp_plan* p, const void* f, const double* mult, c2<T>* ou
     {
       ProfScope _ps(p, "tf.anal.ag", s);
       dim3 ga((unsigned)((nw + PA - 1) / PA), (unsigned)NB2);
-      k_anal_ag<B, T, PA, CPLX><<<ga, 256, smem, s>>>(f, mult, Qg, w0, nw);
+      k_anal_ag<B, T, PA, CPLX><<<ga, Cfg::NT, smem, s>>>(f, mult, Qg, w0, nw);
       HP_CUDA_TRY(cudaGetLastError());
     }
     ProfScope _ps(p, "tf.anal.beta", s);
