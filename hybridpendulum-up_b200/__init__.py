@@ -43,7 +43,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_collision_destroy', 'hp_collision_tables', 'hp_collision_df', 'hp_plan_set_den_model',
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
-           'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info']
+           'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info',
+           'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate']
 
 
 class HPError(RuntimeError):
@@ -140,6 +141,8 @@ def _load():
         'hp_batch_step': [vp, dp, ip, ip],
         'hp_batch_info': [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ip)],
         'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
+        'hp_plan_set_gyro_bias_model': [vp, dp, vp, vp],
+        'hp_gyrobias_propagate': [vp, vp, vp, dp, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -343,6 +346,25 @@ class Plan:
                 raise ValueError('F and f must live in the same memory space')
         _check(_lib.hp_pendulum_propagate_den(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(pf),
                                               ctypes.c_void_p(po), float(dt), METHODS[method.lower()], mi))
+        return out
+
+    def set_gyro_bias_model(self, L: float, G1, G2):
+        """Gyro-bias attitude model of gyro_bias.m:226-300 (3-D plans): bias
+        drift, attitude diffusion G1 and bias random walk G2 on the bias grid of
+        period L (2 in the reference driver)."""
+        g1 = np.ascontiguousarray(np.asarray(G1, float).reshape(3, 3))
+        g2 = np.ascontiguousarray(np.asarray(G2, float).reshape(3, 3))
+        _check(_lib.hp_plan_set_gyro_bias_model(self._h, float(L), g1.ctypes.data, g2.ctypes.data))
+        self.model = dict(L=float(L), G1=g1, G2=g2)
+
+    def gyrobias_propagate(self, F, dt: float, out=None):
+        """Fnew = F + dt dF of the gyro-bias model (one Euler step)."""
+        F = _as_matlab(F, np.complex128)
+        if out is None:
+            out = _empty_like_mem(F, self.F_shape, np.complex128)
+        pi, mi = _ptr(F, np.complex128)
+        po, _ = _ptr(out, np.complex128)
+        _check(_lib.hp_gyrobias_propagate(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), float(dt), mi))
         return out
 
     def density_mf_gauss(self, U, s, V, mu, Sigma):
@@ -697,6 +719,40 @@ def pendulum_propagate_reduced_den32(F, f, X, mR, bt, G, dt, L, u, d, w, method=
     """Mixed-precision twin of pendulum_propagate_reduced_den."""
     plan = _den_plan(F, X, mR, bt, G, L, HP_MIXED)
     return plan.propagate_den(F, f, dt, method)
+
+
+def _bias_period(X, Bx: int) -> float:
+    """Period L of the bias grid behind X = fftn(x) (gyro_bias.m:57-99):
+    x_1 at the first grid point is -L/2; X must be that table."""
+    X = np.asarray(X)
+    L = -2.0 * float(np.real(np.fft.ifftn(X[..., 0]))[0, 0, 0])
+    if not L > 0:
+        raise HPError(HP_ERR_UNSUPPORTED, 'X is not fftn of a uniform grid over [-L/2, L/2)')
+    _check_X(X, Bx, L, 3)
+    return L
+
+
+def _gyrobias_plan(F, X, G1, G2, precision):
+    F = np.asarray(F)
+    if F.ndim != 6:
+        raise HPError(HP_ERR_SHAPE, 'the gyro-bias model has a 3-D bias: F is (2B-1, 2B-1, B, N, N, N)')
+    B, Bx = F.shape[2], F.shape[3] // 2
+    plan = get_plan(B, Bx, 3, precision, HP_REAL)
+    plan.set_gyro_bias_model(_bias_period(X, Bx), G1, G2)
+    return plan
+
+
+def gyrobias_propagate(F, X, dt, u, G1, G2):
+    """Drop-in for the MEX gyrobias_propagate(F,X,dt,u,G1,G2)
+    (propagation/mex/sources/gyrobias_propagate/kernel.cu:8-130) and the
+    integrate function of gyro_bias.m:226-300, FP64.  u is accepted for
+    signature compatibility (the library builds getu.m's matrices itself)."""
+    return _gyrobias_plan(F, X, G1, G2, HP_FP64).gyrobias_propagate(F, dt)
+
+
+def gyrobias_propagate32(F, X, dt, u, G1, G2):
+    """Mixed-precision twin of gyrobias_propagate."""
+    return _gyrobias_plan(F, X, G1, G2, HP_MIXED).gyrobias_propagate(F, dt)
 
 
 def fftSO3R_mex(direction: str, A, d=None, w=None, precision: int = HP_FP64):

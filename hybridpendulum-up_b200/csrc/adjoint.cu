@@ -204,6 +204,7 @@ int axis_md(hp_plan* p, const double2* in, double2* out, int axis, double coef, 
     case 16: return axis_md_launch<16>(p, in, out, axis, coef, s);
     case 20: return axis_md_launch<20>(p, in, out, axis, coef, s);
     case 24: return axis_md_launch<24>(p, in, out, axis, coef, s);
+    case 30: return axis_md_launch<30>(p, in, out, axis, coef, s);
     case 32: return axis_md_launch<32>(p, in, out, axis, coef, s);
     case 40: return axis_md_launch<40>(p, in, out, axis, coef, s);
     case 48: return axis_md_launch<48>(p, in, out, axis, coef, s);
@@ -342,6 +343,7 @@ extern "C" int hp_pendulum_derivative_adjoint(hp_plan* p, const double* lam, dou
   ADJ_CHECK(check_mem(mem));
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   if (p->den_mR) { hp_set_error("the adjoint covers coefficient-gravity models (hp_plan_set_model)"); return HP_ERR_UNSUPPORTED; }
+  if (p->so3d64) { hp_set_error("the adjoint covers the pendulum models (no attitude diffusion)"); return HP_ERR_UNSUPPORTED; }
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   cudaStream_t s = p->stream;
   int st = HP_OK;
@@ -374,6 +376,7 @@ extern "C" int hp_pendulum_adjoint(hp_plan* p, const double* F0, const double* l
   ADJ_CHECK(check_mem(mem));
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   if (p->den_mR) { hp_set_error("the adjoint covers coefficient-gravity models (hp_plan_set_model)"); return HP_ERR_UNSUPPORTED; }
+  if (p->so3d64) { hp_set_error("the adjoint covers the pendulum models (no attitude diffusion)"); return HP_ERR_UNSUPPORTED; }
   if (method != HP_EULER) { hp_set_error("the adjoint covers forward-Euler trajectories"); return HP_ERR_UNSUPPORTED; }
   if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }

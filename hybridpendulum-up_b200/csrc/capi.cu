@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <complex>
 #include <vector>
 #include "common.cuh"
 #include "plan.hpp"
@@ -120,7 +121,7 @@ extern "C" int hp_plan_launch_count(hp_plan* p, long long* count) {
 }
 
 static bool valid_N(int N) {
-  return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 32 || N == 40 ||
+  return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 30 || N == 32 || N == 40 ||
          N == 48 || N == 60;
 }
 static bool valid_B(int B) {
@@ -137,7 +138,7 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
   if (!out) { hp_set_error("plan pointer is null"); return HP_ERR_INVALID; }
   *out = nullptr;
   if (!valid_B(B)) { hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)"); return HP_ERR_INVALID; }
-  if (!valid_N(2 * Bx)) { hp_set_error("2*Bx must be one of 4,6,8,12,16,20,24,32,40,48,60"); return HP_ERR_INVALID; }
+  if (!valid_N(2 * Bx)) { hp_set_error("2*Bx must be one of 4,6,8,12,16,20,24,30,32,40,48,60"); return HP_ERR_INVALID; }
   if (ndim != 2 && ndim != 3) { hp_set_error("ndim must be 2 or 3"); return HP_ERR_INVALID; }
   if (precision != HP_FP64 && precision != HP_MIXED) { hp_set_error("bad precision"); return HP_ERR_INVALID; }
   if (symmetry != HP_REAL && symmetry != HP_COMPLEX) { hp_set_error("bad symmetry"); return HP_ERR_INVALID; }
@@ -250,6 +251,8 @@ extern "C" int hp_plan_set_model(hp_plan* p, const hp_model* m, const double* MR
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   p->model = *m;
   p->den_mR = nullptr;
+  p->so3d64 = nullptr;
+  p->so3d32 = nullptr;
   p->has_model = true;
   return HP_OK;
 }
@@ -282,6 +285,78 @@ extern "C" int hp_plan_set_den_model(hp_plan* p, const hp_model* m, const double
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   p->model = *m;
   p->den_mR = d;
+  p->so3d64 = nullptr;
+  p->so3d32 = nullptr;
+  p->has_model = true;
+  return HP_OK;
+}
+
+// Attitude-diffusion weights of the gyro-bias model (gyro_bias.m:274-283):
+//   sum_ij G1_ij F^l u_i^T u_j^T = F^l K^T,  K = sum_ij G1_ij u_j u_i,
+// so output (l, m, n) takes K[n][k] F^l_{m,k} for k = n-2..n+2 (u_1, u_2 are
+// bidiagonal in n and u_3 is diagonal).  u as in getu.m:132-163:
+//   u_1[n-1][n] = -i/2 sqrt((l+n)(l-n+1)),  u_1[n+1][n] = -i/2 sqrt((l-n)(l+n+1)),
+//   u_2[n-1][n] =  1/2 sqrt((l+n)(l-n+1)),  u_2[n+1][n] = -1/2 sqrt((l-n)(l+n+1)),
+//   u_3[n][n]   = -i n.
+static std::complex<double> getu_entry(int l, int a, int b, int i) {
+  using cd = std::complex<double>;
+  if (a < -l || a > l || b < -l || b > l) return cd(0, 0);
+  if (i == 2) return a == b ? cd(0, -a) : cd(0, 0);
+  if (a == b - 1) {
+    const double v = 0.5 * std::sqrt((double)(l + b) * (l - b + 1));
+    return i == 0 ? cd(0, -v) : cd(v, 0);
+  }
+  if (a == b + 1) {
+    const double v = 0.5 * std::sqrt((double)(l - b) * (l + b + 1));
+    return i == 0 ? cd(0, -v) : cd(-v, 0);
+  }
+  return cd(0, 0);
+}
+
+extern "C" int hp_plan_set_gyro_bias_model(hp_plan* p, double L, const double* G1, const double* G2) {
+  if (!p || !G1 || !G2) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (p->ndim != 3) { hp_set_error("the gyro-bias model has a 3-D bias (ndim = 3)"); return HP_ERR_UNSUPPORTED; }
+  if (!(L > 0) || !std::isfinite(L)) { hp_set_error("L must be positive"); return HP_ERR_INVALID; }
+  for (int e = 0; e < 9; ++e)
+    if (!std::isfinite(G1[e]) || !std::isfinite(G2[e])) { hp_set_error("G1/G2 have non-finite entries"); return HP_ERR_NONFINITE; }
+  using cd = std::complex<double>;
+  std::vector<double2> w64((size_t)p->nrows * 5);
+  std::vector<float2> w32((size_t)p->nrows * 5);
+  for (long long r = 0; r < p->nrows; ++r) {
+    const int l = p->h_rows[r].x, n = p->h_rows[r].z;
+    for (int o = 0; o < 5; ++o) {
+      const int k = n + o - 2;
+      cd K(0, 0);
+      if (k >= -l && k <= l)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            if (G1[i * 3 + j] == 0.0) continue;
+            cd uu(0, 0);   // (u_j u_i)[n][k]
+            for (int q = std::max(-l, n - 1); q <= std::min(l, n + 1); ++q) uu += getu_entry(l, n, q, j) * getu_entry(l, q, k, i);
+            K += G1[i * 3 + j] * uu;
+          }
+      w64[(size_t)r * 5 + o] = make_double2(K.real(), K.imag());
+      w32[(size_t)r * 5 + o] = make_float2((float)K.real(), (float)K.imag());
+    }
+  }
+  int st = HP_OK;
+  double2* d64 = (double2*)p->ws_get("model.so3d64", sizeof(double2) * w64.size(), &st);
+  if (st) return st;
+  float2* d32 = (float2*)p->ws_get("model.so3d32", sizeof(float2) * w32.size(), &st);
+  if (st) return st;
+  HP_CUDA_TRY(cudaMemcpy(d64, w64.data(), sizeof(double2) * w64.size(), cudaMemcpyHostToDevice));
+  HP_CUDA_TRY(cudaMemcpy(d32, w32.data(), sizeof(float2) * w32.size(), cudaMemcpyHostToDevice));
+  HP_CHECK(hp_build_gravity_taps(p));
+  for (int n2 = 0; n2 < 3; ++n2)
+    for (int i = 0; i < 3; ++i) p->mr1[n2][i] = make_double2(0.0, 0.0);   // no gravity
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  hp_model m{};
+  m.L = L;
+  for (int e = 0; e < 9; ++e) m.G[e] = G2[e];   // bias random walk (gyro_bias.m:285-297)
+  p->model = m;                                  // b = 0, no gyroscopic term
+  p->den_mR = nullptr;
+  p->so3d64 = d64;
+  p->so3d32 = d32;
   p->has_model = true;
   return HP_OK;
 }
@@ -433,6 +508,12 @@ extern "C" int hp_pendulum_propagate(hp_plan* p, const double* Fold, double* Fne
   HP_CHECK(finish_out(p, Fnew, dOut, fb, mem));
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HP_OK;
+}
+
+extern "C" int hp_gyrobias_propagate(hp_plan* p, const double* Fold, double* Fnew, double dt, int mem) {
+  if (!p) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  if (!p->has_model || !p->so3d64) { hp_set_error("no gyro-bias model: call hp_plan_set_gyro_bias_model first"); return HP_ERR_NO_MODEL; }
+  return hp_pendulum_propagate(p, Fold, Fnew, dt, HP_EULER, mem);
 }
 
 extern "C" int hp_pendulum_propagate_den(hp_plan* p, const double* Fold, const double* f, double* Fnew,

@@ -80,7 +80,8 @@ template <typename T> __host__ __device__ constexpr size_t local_tile_bytes(int 
 template <typename T, int W, int NDIM>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __restrict__ F,
                                                c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
-                                               const c2<T>* __restrict__ Gx, DerivParams prm) {
+                                               const c2<T>* __restrict__ Gx, const c2<T>* __restrict__ sdk,
+                                               DerivParams prm) {
   using C = c2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int D = 2 * L.lmax + 1;
@@ -173,6 +174,19 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
       ax += nu[n2o].x * sx - nu[n2o].y * sy;
       ay += nu[n2o].x * sy + nu[n2o].y * sx;
     }
+    if (sdk) {  // attitude diffusion: sum_o K^l[n][n+o-2] F^l_{m, n+o-2} (gyro-bias model)
+      const c2<T>* kw = sdk + (size_t)(r0 + r) * 5;
+#pragma unroll
+      for (int o = 0; o < 5; ++o) {
+        const int k = n + o - 2;
+        if (k < -l || k > l) continue;
+        const int ak = abs(k);
+        const C fs = tile[(sseg[k + lmax] - (am > ak ? am : ak) + l) * W + w];
+        const C wk = kw[o];
+        ax += wk.x * fs.x - wk.y * fs.y;
+        ay += wk.x * fs.y + wk.y * fs.x;
+      }
+    }
     if (Gx) {  // density-side gravity term (density-gravity models)
       const C gx = Gx[(size_t)(r0 + r) * L.nx + wg];
       ax += gx.x;
@@ -192,6 +206,9 @@ template <typename T> static size_t local_smem(const hp_plan* p, int W) {
 template <typename T> static const T* tap_table(const hp_plan* p);
 template <> const double* tap_table<double>(const hp_plan* p) { return p->tap_wr; }
 template <> const float* tap_table<float>(const hp_plan* p) { return p->tap_wr32; }
+template <typename T> static const c2<T>* so3d_table(const hp_plan* p);
+template <> const double2* so3d_table<double>(const hp_plan* p) { return p->so3d64; }
+template <> const float2* so3d_table<float>(const hp_plan* p) { return p->so3d32; }
 
 template <typename T> static constexpr int local_w() { return sizeof(T) == 8 ? 16 : 32; }
 
@@ -486,10 +503,10 @@ static int local_w_launch(hp_plan* p, const double2* F, c2<T>* G, const c2<T>* G
   ProfScope _ps(p, "deriv.local", s);
   if (p->ndim == 3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 3><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, prm);
+    k_local<T, W, 3><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 2><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, prm);
+    k_local<T, W, 2><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -664,10 +681,11 @@ static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a
     case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 30: return run_deriv_N<30, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     case 40: case 48: case 60: return run_deriv_lines<T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     default:
-      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24, 30 or 32)");
       return HP_ERR_UNSUPPORTED;
   }
 }
@@ -857,9 +875,10 @@ static int noalloc_T(hp_plan* p, const double2* F, double2* dF, unsigned char* b
     case 16: return noalloc_N<16, T>(p, F, dF, base, prm);
     case 20: return noalloc_N<20, T>(p, F, dF, base, prm);
     case 24: return noalloc_N<24, T>(p, F, dF, base, prm);
+    case 30: return noalloc_N<30, T>(p, F, dF, base, prm);
     case 32: return noalloc_N<32, T>(p, F, dF, base, prm);
     default:
-      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24 or 32)");
+      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24, 30 or 32)");
       return HP_ERR_UNSUPPORTED;
   }
 }

@@ -60,6 +60,10 @@ struct hp_plan {
   float* tap_wr32 = nullptr;
   double2 mr1[3][3] = {};    // MR_i^1_{0 n2} of the model: [n2+1][i]
   double* den_mR = nullptr;  // [2][(2B)^3] density-side gravity multipliers (pendulum_reduced_den)
+  // attitude diffusion sum_ij G1_ij F^l u_i^T u_j^T of the gyro-bias model:
+  // [row][5] complex weights of F^l_{m, n+o-2}, o = 0..4 (null when absent)
+  double2* so3d64 = nullptr;
+  float2* so3d32 = nullptr;
 
   // profiling
   bool prof_on = false;

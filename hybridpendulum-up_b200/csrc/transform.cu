@@ -339,12 +339,13 @@ static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cu
     case 16: return omega_fft<16, Tin, T>(p, in, out, inv, s);
     case 20: return omega_fft<20, Tin, T>(p, in, out, inv, s);
     case 24: return omega_fft<24, Tin, T>(p, in, out, inv, s);
+    case 30: return omega_fft<30, Tin, T>(p, in, out, inv, s);
     case 32: return omega_fft<32, Tin, T>(p, in, out, inv, s);
     case 40: return omega_fft<40, Tin, T>(p, in, out, inv, s);
     case 48: return omega_fft<48, Tin, T>(p, in, out, inv, s);
     case 60: return omega_fft<60, Tin, T>(p, in, out, inv, s);
     default:
-      hp_set_error("omega grid size 2Bx not supported (4, 6, 8, 12, 16, 20, 24, 32, 40, 48, 60)");
+      hp_set_error("omega grid size 2Bx not supported (4, 6, 8, 12, 16, 20, 24, 30, 32, 40, 48, 60)");
       return HP_ERR_UNSUPPORTED;
   }
 }

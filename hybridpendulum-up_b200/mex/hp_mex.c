@@ -6,6 +6,7 @@
  *   mex -R2018a -DHP_MEX_PROPAGATE3 -DHP_MEX_MIXED -output pendulum_propagate32 hp_mex.c ...
  *   mex -R2018a -DHP_MEX_PROPAGATE2 -output pendulum_propagate_reduced hp_mex.c ...
  *   mex -R2018a -DHP_MEX_FFTSO3R    -output fftSO3R_mex                hp_mex.c ...
+ *   mex -R2018a -DHP_MEX_GYROBIAS   -output gyrobias_propagate         hp_mex.c ...
  *
  * Signatures (unchanged from the reference):
  *   Fnew = pendulum_propagate(F,X,OJO,MR,bt,G,dt,L,u,CG,method)
@@ -14,6 +15,8 @@
  *          (propagation/mex/sources/pendulum_propagate_reduced/kernel.cu:16-74)
  *   F = fftSO3R_mex('forward',f,d,w) ; f = fftSO3R_mex('backward',F,d)
  *          (propagation/mex/sources/fftSO3R/kernel.cu:8-19, 197-202)
+ *   Fnew = gyrobias_propagate(F,X,dt,u,G1,G2)
+ *          (propagation/mex/sources/gyrobias_propagate/kernel.cu:8-130)
  * u, CG, d and w are accepted and ignored: the library builds the same tables on
  * the device.  X is taken as fftn of the uniform grid of period L; OJO is reduced
  * to the diagonal-J coefficients (g1 x2 x3, g2 x1 x3, g3 x1 x2) by an inverse
@@ -64,7 +67,7 @@ static int method_code(const mxArray* a) {
   return -1;
 }
 
-#if defined(HP_MEX_PROPAGATE3) || defined(HP_MEX_PROPAGATE2)
+#if defined(HP_MEX_PROPAGATE3) || defined(HP_MEX_PROPAGATE2) || defined(HP_MEX_GYROBIAS)
 /* ifftn of one N^3 component by separable 1-D inverse DFTs (real part kept). */
 static void ifft3_real(const mxComplexDouble* X, int N, double* out) {
   const size_t n3 = (size_t)N * N * N;
@@ -95,6 +98,9 @@ static void ifft3_real(const mxComplexDouble* X, int N, double* out) {
   mxFree(re); mxFree(im); mxFree(tr); mxFree(ti);
 }
 
+#endif
+
+#if defined(HP_MEX_PROPAGATE3) || defined(HP_MEX_PROPAGATE2)
 /* (g1, g2, g3) with ifftn(OJO_i) = g_i * x_j * x_k on the grid x = -L/2 + L*idx/N. */
 static void fit_gyro(const mxArray* OJO, int N, double L, double g[3]) {
   const size_t n3 = (size_t)N * N * N;
@@ -184,6 +190,36 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   } else {
     mexErrMsgIdAndTxt("hp:direction", "direction must be 'forward' or 'backward'");
   }
+  (void)nlhs;
+}
+#endif
+
+#ifdef HP_MEX_GYROBIAS
+/* The bias grid period L is read off X = fftn(x) (gyro_bias.m:68-99): x_1 at
+ * the first grid point is -L/2. */
+void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  if (nrhs != 6) mexErrMsgIdAndTxt("hp:nrhs", "expected 6 inputs (F,X,dt,u,G1,G2)");
+  const mxArray* F = prhs[0];
+  if (!mxIsComplex(F) || !mxIsDouble(F)) mexErrMsgIdAndTxt("hp:F", "F must be complex double");
+  if (mxGetNumberOfDimensions(F) != 6) mexErrMsgIdAndTxt("hp:F", "F has the wrong rank");
+  const mwSize* dims = mxGetDimensions(F);
+  const int B = (int)dims[2], Bx = (int)dims[3] / 2, N = 2 * Bx;
+  const mxComplexDouble* X = mxGetComplexDoubles(prhs[1]);
+  if (!X) mexErrMsgIdAndTxt("hp:X", "X must be complex double");
+  double* x1 = mxMalloc(sizeof(double) * (size_t)N * N * N);
+  ifft3_real(X, N, x1);
+  const double L = -2.0 * x1[0];
+  mxFree(x1);
+  const double* G1 = mxGetDoubles(prhs[4]);
+  const double* G2 = mxGetDoubles(prhs[5]);
+  double g1[9], g2[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) { g1[i * 3 + j] = G1[i + 3 * j]; g2[i * 3 + j] = G2[i + 3 * j]; }
+  hp_plan* p = plan_for(B, Bx, 3, HP_MEX_PRECISION, HP_REAL);
+  check(hp_plan_set_gyro_bias_model(p, L, g1, g2));
+  plhs[0] = mxCreateUninitNumericArray(6, (size_t*)dims, mxDOUBLE_CLASS, mxCOMPLEX);
+  check(hp_gyrobias_propagate(p, (const double*)mxGetComplexDoubles(F), (double*)mxGetComplexDoubles(plhs[0]),
+                              mxGetScalar(prhs[2]), HP_HOST));
   (void)nlhs;
 }
 #endif

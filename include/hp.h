@@ -149,6 +149,25 @@ int hp_plan_set_den_model(hp_plan* plan, const hp_model* model, const double* mR
 int hp_pendulum_propagate_den(hp_plan* plan, const double* Fold, const double* f, double* Fnew,
                               double dt, int method, int mem);
 
+/* Gyro-bias attitude model: the inputs of the MEX
+ * gyrobias_propagate(F,X,dt,u,G1,G2)
+ * (propagation/mex/sources/gyrobias_propagate/kernel.cu:8-130) and of the
+ * integrate function of gyro_bias.m:226-300.  The state is (R, x) with x the
+ * 3-D gyro bias on the grid x_i = -L/2 + L*j/(2Bx) (gyro_bias.m:57-66 has
+ * L = 2), and
+ *   dF = -sum_i F_omega[x_i f]^l (u^l_i)^T            bias drift (226-265)
+ *        + sum_ij G1_ij F^l (u^l_i)^T (u^l_j)^T        gyro random walk (268-279)
+ *        + sum_ij G2_ij c_ij F                         bias random walk (281-297)
+ * with c_ij the diffusion multipliers of hp_model for period L (the reference
+ * writes them with pi = 2 pi / L at L = 2).  G1, G2: row-major 3x3, host.
+ * Needs ndim = 3; replaces any other model of the plan (and is replaced by
+ * hp_plan_set_model / hp_plan_set_den_model).  hp_pendulum_propagate,
+ * hp_pendulum_derivative and the state API then run this model; the adjoint
+ * entry points return HP_ERR_UNSUPPORTED for it. */
+int hp_plan_set_gyro_bias_model(hp_plan* plan, double L, const double* G1, const double* G2);
+/* Fnew = Fold + dt dF (the Euler step of gyro_bias.m:299 and the MEX). */
+int hp_gyrobias_propagate(hp_plan* plan, const double* Fold, double* Fnew, double dt, int mem);
+
 /* ---- reverse mode (no counterpart in the reference) ----
  * Gradients of a scalar loss L(F_T) of a forward-Euler trajectory
  * F_{n+1} = F_n + dt A F_n (hp_pendulum_propagate with HP_EULER), with the
