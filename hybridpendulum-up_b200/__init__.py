@@ -92,7 +92,7 @@ def _mfg_args(U, s, V, mu, Sigma, ndim):
 class hp_collision_params(ctypes.Structure):
     _fields_ = [('d', ctypes.c_double), ('h', ctypes.c_double), ('r', ctypes.c_double),
                 ('theta_t', ctypes.c_double), ('lambda_max', ctypes.c_double), ('epsilon', ctypes.c_double),
-                ('L', ctypes.c_double), ('Gd', ctypes.c_double * 4), ('nD', ctypes.c_int)]
+                ('L', ctypes.c_double), ('Gd', ctypes.c_double * 9), ('nD', ctypes.c_int)]
 
 
 class hp_plan_info_t(ctypes.Structure):
@@ -526,13 +526,15 @@ def _empty_like_mem(ref, shape, dtype):
 class Collision:
     """Hybrid collision operator of pendulum_reduced_hybrid on a 2-D plan:
     getLambda_mex + getOmega_mex('new') + getFcL_mex tables, and the per-step
-    pendulum_reduced_discrete_propagate(true, f, ...)."""
+    pendulum_reduced_discrete_propagate(true, f, ...).  On a 3-D plan the same
+    operator on a 3-D Omega grid (Gd then 3x3)."""
 
     def __init__(self, plan: Plan, d, h, r, theta_t, lambda_max, epsilon, L, Gd, nD=10):
         p = hp_collision_params()
         p.d, p.h, p.r, p.theta_t, p.lambda_max, p.epsilon, p.L = d, h, r, theta_t, lambda_max, epsilon, L
-        g = np.asarray(Gd, float).reshape(2, 2).ravel(order='F')
-        for i in range(4):
+        nd = plan.ndim
+        g = np.asarray(Gd, float).reshape(nd, nd).ravel(order='F')
+        for i in range(nd * nd):
             p.Gd[i] = g[i]
         p.nD = int(nD)
         hnd, n = ctypes.c_void_p(), ctypes.c_int()
@@ -546,9 +548,9 @@ class Collision:
             self._h = None
 
     def tables(self):
-        nx = self.plan.N ** 2
+        nx = self.plan.N ** self.plan.ndim
         k, nD = self.numR, self.nD
-        lam = np.zeros((nx, k)); ind = np.zeros(k, np.int32); om = np.zeros((nx, k, 2))
+        lam = np.zeros((nx, k)); ind = np.zeros(k, np.int32); om = np.zeros((nx, k, self.plan.ndim))
         fcL = np.zeros((nx, k, nD)); idx = np.zeros((nx, k, nD), np.int16)
         PC = np.zeros((8 * self.plan.B ** 3, 3))
         ptrs = [ctypes.c_void_p(a.ctypes.data) for a in (lam, ind, om, fcL, idx, PC)]

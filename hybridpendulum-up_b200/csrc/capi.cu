@@ -689,7 +689,7 @@ extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int
   if (!s || !c || nsteps < 0) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
   hp_plan* p = s->plan;
   if (hp_collision_plan(c) != p) { hp_set_error("collision operator belongs to another plan"); return HP_ERR_INVALID; }
-  if (!p->has_model || !p->den_mR) { hp_set_error("no density-gravity model: call hp_plan_set_den_model first"); return HP_ERR_NO_MODEL; }
+  if (!p->has_model) { hp_set_error("no model: call hp_plan_set_den_model or hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
   if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
   cudaStream_t st = p->stream;

@@ -1,12 +1,19 @@
-// Hybrid collision operator of pendulum_reduced_hybrid (2-D reduced Omega):
+// Hybrid collision operator of pendulum_reduced_hybrid (2-D reduced Omega,
+// and its extension to a 3-D Omega grid):
 // switching rate lambda(R, x), reset map Omega+, truncated Gaussian kernel fcL
 // and the per-step update df = sum_d fcL f(R, idx) - lambda f (FP64, as the
 // reference).  Follows propagation/discrete/mex/sources/pendulum_reduced_collision:
 // getLambda.cu:8-85,192-267, getOmega.cu:64-103, getFcL.cu:11-166,
 // propagate.cu:6-121,181-231.
 //
+// 3-D Omega (no reference counterpart: the reference builds the 2-D reduced
+// model only, getOmega.cu:86-96 takes Omega = [x1, x2, 0]): the same
+// kinematics with all three components, omega = R Omega, the reset acting on
+// the (2, 3) components of omega as in 2-D, Omega+ = R^T omega+ in R^3 and a
+// 3-D Gaussian of covariance Gd (3x3) for the landing kernel.
+//
 // Layouts (those of the reference MEX):
-//   f, df         [ix][iR]      ix = i + 2Bx j, iR = a + 2B b + 4B^2 c
+//   f, df         [ix][iR]      ix = i + 2Bx j (+ 4Bx^2 k), iR = a + 2B b + 4B^2 c
 //   lambda        [ix][k]       k indexes the colliding attitudes indR
 //   fcL, fcL_idx  [ix][k][d]    d < nD
 #include <cmath>
@@ -20,7 +27,7 @@ struct CollisionTables {
   int numR = 0, nD = 0;
   int* indR = nullptr;        // [numR]
   double* lambda = nullptr;   // [nx][numR]
-  double* omega = nullptr;    // [nx][numR][2]
+  double* omega = nullptr;    // [nx][numR][ndim]
   double* fcL = nullptr;      // [nx][numR][nD]
   short* idx = nullptr;       // [nx][numR][nD]
   double* PC = nullptr;       // [nR][3]
@@ -61,53 +68,65 @@ __global__ void k_coll_theta(int B, int nR, double theta0, double thetat, double
 }
 
 // lambda(ix, k) and Omega+(ix, k) for the colliding attitudes.
+template <int NDIM>
 __global__ void k_coll_lambda_omega(int B, int N, double L, int numR, const int* __restrict__ indR,
                                     const char* __restrict__ cat, const double* __restrict__ theta,
                                     const double* __restrict__ PC, double theta0, double thetat, double lmax,
                                     double eps, double* __restrict__ lambda, double* __restrict__ omega) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nx = N * N;
+  const int nx = NDIM == 3 ? N * N * N : N * N;
   if (t >= (long long)nx * numR) return;
   const int k = (int)(t % numR), ix = (int)(t / numR);
   const int iR = indR[k];
   double R[3][3];
   rot_of(iR, B, R);
-  const double x1 = -L / 2 + L / N * (ix % N), x2 = -L / 2 + L / N * (ix / N);
+  const double x1 = -L / 2 + L / N * (ix % N), x2 = -L / 2 + L / N * ((ix / N) % N);
+  const double x3 = NDIM == 3 ? -L / 2 + L / N * (ix / (N * N)) : 0.0;
   double lam = cat[iR] == 2 ? lmax : lmax / 2 * sin(M_PI / (2 * thetat) * (theta[iR] - theta0)) + lmax / 2;
   if (cat[iR] == 0) lam = 0.0;
-  const double o0 = R[1][0] * x1 + R[1][1] * x2, o1 = R[2][0] * x1 + R[2][1] * x2;
-  const double vC = o0 * PC[3 * iR + 2] - o1 * PC[3 * iR + 1];
+  // omega = R Omega (spatial angular velocity); contact-point velocity along the wall normal
+  const double w0 = R[0][0] * x1 + R[0][1] * x2 + R[0][2] * x3;
+  double w1 = R[1][0] * x1 + R[1][1] * x2 + R[1][2] * x3;
+  double w2 = R[2][0] * x1 + R[2][1] * x2 + R[2][2] * x3;
+  const double vC = w1 * PC[3 * iR + 2] - w2 * PC[3 * iR + 1];
   lambda[t] = vC < 0.0 ? 0.0 : lam;
   // reset map
   const double nt = sqrt(R[1][2] * R[1][2] + R[2][2] * R[2][2]);
   const double t1 = R[2][2] / nt, t2 = -R[1][2] / nt;
-  const double w0 = R[0][0] * x1 + R[0][1] * x2;
-  double w1 = R[1][0] * x1 + R[1][1] * x2, w2 = R[2][0] * x1 + R[2][1] * x2;
   const double ot = (1.0 + eps) * (w1 * t1 + w2 * t2);
   w1 -= ot * t1;
   w2 -= ot * t2;
-  omega[2 * t] = R[0][0] * w0 + R[1][0] * w1 + R[2][0] * w2;
-  omega[2 * t + 1] = R[0][1] * w0 + R[1][1] * w1 + R[2][1] * w2;
+#pragma unroll
+  for (int c = 0; c < NDIM; ++c) omega[NDIM * t + c] = R[0][c] * w0 + R[1][c] * w1 + R[2][c] * w2;
 }
+
+// inverse covariance (symmetric part) and normaliser of the landing Gaussian
+struct GaussQ { double i00, i01, i02, i11, i12, i22, cn; };
 
 // Largest nD Gaussian taps per (landing point ix1, attitude k), ties keeping the
 // lower source index first (the stable descending sort of getFcL.cu:76).
-template <int MAXD>
-__global__ void k_coll_topd(int N, double L, int numR, int nD, const double* __restrict__ omega, double i00,
-                            double i01, double i11, double cn, double* __restrict__ fcL, short* __restrict__ idx) {
+template <int MAXD, int NDIM>
+__global__ void k_coll_topd(int N, double L, int numR, int nD, const double* __restrict__ omega, GaussQ g,
+                            double* __restrict__ fcL, short* __restrict__ idx) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int nx = N * N;
+  const int nx = NDIM == 3 ? N * N * N : N * N;
   if (t >= (long long)nx * numR) return;
   const int k = (int)(t % numR), ix1 = (int)(t / numR);
-  const double x1 = -L / 2 + L / N * (ix1 % N), x2 = -L / 2 + L / N * (ix1 / N);
+  const double x1 = -L / 2 + L / N * (ix1 % N), x2 = -L / 2 + L / N * ((ix1 / N) % N);
+  const double x3 = NDIM == 3 ? -L / 2 + L / N * (ix1 / (N * N)) : 0.0;
   double v[MAXD];
   int id[MAXD];
   int cnt = 0;
   for (int ix2 = 0; ix2 < nx; ++ix2) {
-    const double d0 = x1 - omega[2 * ((long long)ix2 * numR + k)];
-    const double d1 = x2 - omega[2 * ((long long)ix2 * numR + k) + 1];
-    const double q = i00 * d0 * d0 + i01 * d0 * d1 + i11 * d1 * d1;
-    const double fc = exp(-0.5 * q) * cn;
+    const double* o = omega + NDIM * ((long long)ix2 * numR + k);
+    const double d0 = x1 - o[0];
+    const double d1 = x2 - o[1];
+    double q = g.i00 * d0 * d0 + g.i01 * d0 * d1 + g.i11 * d1 * d1;
+    if (NDIM == 3) {
+      const double d2 = x3 - o[2];
+      q += g.i02 * d0 * d2 + g.i12 * d1 * d2 + g.i22 * d2 * d2;
+    }
+    const double fc = exp(-0.5 * q) * g.cn;
     if (cnt < nD || fc > v[nD - 1]) {
       int p = cnt < nD ? cnt++ : nD - 1;      // insertion position from the end
       while (p > 0 && v[p - 1] < fc) {         // strict: equal values keep the earlier index first
@@ -133,13 +152,13 @@ __global__ void k_coll_norm(int nx, int numR, int nD, const double* __restrict__
   atomicAdd(&norm[(long long)idx[t] * numR + k], fcL[t]);
 }
 
-__global__ void k_coll_scale(int nx, int numR, int nD, double dx2, const double* __restrict__ norm,
+__global__ void k_coll_scale(int nx, int numR, int nD, double dxn, const double* __restrict__ norm,
                              const double* __restrict__ lambda, double* __restrict__ fcL, const short* __restrict__ idx) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)nx * numR * nD) return;
   const int k = (int)((t / nD) % numR);
   const long long src = (long long)idx[t] * numR + k;
-  fcL[t] = fcL[t] / (norm[src] * dx2) * (lambda[src] * dx2);
+  fcL[t] = fcL[t] / (norm[src] * dxn) * (lambda[src] * dxn);
 }
 
 // df(R_k, x) = sum_d fcL f(R_k, idx) - lambda f(R_k, x); rows of non-colliding
@@ -176,10 +195,10 @@ struct hp_collision {
 extern "C" int hp_collision_create(hp_plan* p, const hp_collision_params* prm, hp_collision** out, int* numR) {
   if (!p || !prm || !out) { hp_set_error("null argument"); return HP_ERR_INVALID; }
   *out = nullptr;
-  if (p->ndim != 2) { hp_set_error("the collision operator is defined for the 2-D reduced model"); return HP_ERR_UNSUPPORTED; }
   if (prm->nD < 1 || prm->nD > 32) { hp_set_error("nD must be in 1..32"); return HP_ERR_INVALID; }
   if (!(prm->L > 0) || !(prm->theta_t > 0)) { hp_set_error("bad collision parameters"); return HP_ERR_INVALID; }
-  const int B = p->B, N = p->N, nR = 8 * B * B * B, nx = N * N;
+  const int B = p->B, N = p->N, nR = 8 * B * B * B, nx = (int)p->nx, nd = p->ndim;
+  if (nx > 32768) { hp_set_error("the tap indices are 16-bit: at most 32768 omega points"); return HP_ERR_UNSUPPORTED; }
   cudaStream_t s = p->stream;
   const double hr = std::sqrt(prm->h * prm->h + prm->r * prm->r);
   const double theta0 = std::asin(prm->d / hr) - std::asin(prm->r / hr);
@@ -216,7 +235,7 @@ extern "C" int hp_collision_create(hp_plan* p, const hp_collision_params* prm, h
   double* norm = nullptr;
   if (cudaMalloc(&c->t.indR, sizeof(int) * nk) != cudaSuccess ||
       cudaMalloc(&c->t.lambda, sizeof(double) * nxk) != cudaSuccess ||
-      cudaMalloc(&c->t.omega, sizeof(double) * 2 * nxk) != cudaSuccess ||
+      cudaMalloc(&c->t.omega, sizeof(double) * nd * nxk) != cudaSuccess ||
       cudaMalloc(&c->t.fcL, sizeof(double) * nxk * prm->nD) != cudaSuccess ||
       cudaMalloc(&c->t.idx, sizeof(short) * nxk * prm->nD) != cudaSuccess ||
       cudaMalloc(&norm, sizeof(double) * nxk) != cudaSuccess) {
@@ -229,20 +248,46 @@ extern "C" int hp_collision_create(hp_plan* p, const hp_collision_params* prm, h
   const unsigned g1 = (unsigned)((nxk + 127) / 128);
   {
     ProfScope _ps(p, "coll.setup", s);
-    k_coll_lambda_omega<<<g1, 128, 0, s>>>(B, N, prm->L, nk, c->t.indR, cat, theta, c->t.PC, theta0, prm->theta_t,
-                                           prm->lambda_max, prm->epsilon, c->t.lambda, c->t.omega);
+    if (nd == 3)
+      k_coll_lambda_omega<3><<<g1, 128, 0, s>>>(B, N, prm->L, nk, c->t.indR, cat, theta, c->t.PC, theta0, prm->theta_t,
+                                                prm->lambda_max, prm->epsilon, c->t.lambda, c->t.omega);
+    else
+      k_coll_lambda_omega<2><<<g1, 128, 0, s>>>(B, N, prm->L, nk, c->t.indR, cat, theta, c->t.PC, theta0, prm->theta_t,
+                                                prm->lambda_max, prm->epsilon, c->t.lambda, c->t.omega);
   }
-  // Gaussian of covariance Gd (column-major 2x2)
-  const double g00 = prm->Gd[0], g10 = prm->Gd[1], g01 = prm->Gd[2], g11 = prm->Gd[3];
-  const double det = g00 * g11 - g01 * g10;
-  if (!(det > 0)) { cudaFree(norm); hp_set_error("Gd must be positive definite"); return fail(HP_ERR_INVALID); }
-  const double cn = 1.0 / (2 * M_PI * std::sqrt(det));
-  const double i00 = g11 / det, i01 = (-g01 - g10) / det, i11 = g00 / det;
+  // Gaussian of covariance Gd (column-major nd x nd): q = d^T Gd^-1 d with the
+  // cross terms of the symmetric part folded (i01 = (inv01 + inv10), ...)
+  GaussQ g{};
+  {
+    const double* G = prm->Gd;
+    double inv[3][3] = {}, det = 0;
+    if (nd == 2) {
+      const double g00 = G[0], g10 = G[1], g01 = G[2], g11 = G[3];
+      det = g00 * g11 - g01 * g10;
+      inv[0][0] = g11 / det; inv[0][1] = -g01 / det; inv[1][0] = -g10 / det; inv[1][1] = g00 / det;
+    } else {
+      auto at = [&](int i, int j) { return G[i + 3 * j]; };
+      const double c00 = at(1, 1) * at(2, 2) - at(1, 2) * at(2, 1), c01 = at(1, 2) * at(2, 0) - at(1, 0) * at(2, 2),
+                   c02 = at(1, 0) * at(2, 1) - at(1, 1) * at(2, 0);
+      det = at(0, 0) * c00 + at(0, 1) * c01 + at(0, 2) * c02;
+      // inverse = adjugate / det (adj[j][i] = cofactor[i][j])
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          const int a0 = (j + 1) % 3, a1 = (j + 2) % 3, b0 = (i + 1) % 3, b1 = (i + 2) % 3;
+          inv[i][j] = (at(a0, b0) * at(a1, b1) - at(a0, b1) * at(a1, b0)) / det;
+        }
+    }
+    if (!(det > 0) || !std::isfinite(det)) { cudaFree(norm); hp_set_error("Gd must be positive definite"); return fail(HP_ERR_INVALID); }
+    g.i00 = inv[0][0]; g.i01 = inv[0][1] + inv[1][0]; g.i11 = inv[1][1];
+    g.i02 = inv[0][2] + inv[2][0]; g.i12 = inv[1][2] + inv[2][1]; g.i22 = inv[2][2];
+    g.cn = 1.0 / (std::pow(2 * M_PI, 0.5 * nd) * std::sqrt(det));
+  }
   {
     ProfScope _ps(p, "coll.setup", s);
-    k_coll_topd<32><<<g1, 128, 0, s>>>(N, prm->L, nk, prm->nD, c->t.omega, i00, i01, i11, cn, c->t.fcL, c->t.idx);
+    if (nd == 3) k_coll_topd<32, 3><<<g1, 128, 0, s>>>(N, prm->L, nk, prm->nD, c->t.omega, g, c->t.fcL, c->t.idx);
+    else k_coll_topd<32, 2><<<g1, 128, 0, s>>>(N, prm->L, nk, prm->nD, c->t.omega, g, c->t.fcL, c->t.idx);
   }
-  const double dx = prm->L / N, dx2 = dx * dx;
+  const double dx = prm->L / N, dx2 = nd == 3 ? dx * dx * dx : dx * dx;
   HP_CUDA_TRY(cudaMemsetAsync(norm, 0, sizeof(double) * nxk, s));
   const unsigned g2 = (unsigned)((nxk * prm->nD + 127) / 128);
   {
@@ -274,11 +319,11 @@ extern "C" int hp_collision_tables(hp_collision* c, double* lambda, int* indR, d
   if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("bad mem"); return HP_ERR_INVALID; }
   hp_plan* p = c->plan;
   const cudaMemcpyKind kind = mem == HP_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  const size_t nxk = (size_t)p->N * p->N * c->t.numR;
+  const size_t nxk = (size_t)p->nx * c->t.numR;
   const int nR = 8 * p->B * p->B * p->B;
   if (lambda && nxk) HP_CUDA_TRY(cudaMemcpy(lambda, c->t.lambda, sizeof(double) * nxk, kind));
   if (indR && c->t.numR) HP_CUDA_TRY(cudaMemcpy(indR, c->t.indR, sizeof(int) * c->t.numR, kind));
-  if (omega && nxk) HP_CUDA_TRY(cudaMemcpy(omega, c->t.omega, sizeof(double) * 2 * nxk, kind));
+  if (omega && nxk) HP_CUDA_TRY(cudaMemcpy(omega, c->t.omega, sizeof(double) * p->ndim * nxk, kind));
   if (fcL && nxk) HP_CUDA_TRY(cudaMemcpy(fcL, c->t.fcL, sizeof(double) * nxk * c->t.nD, kind));
   if (fcL_indx && nxk) HP_CUDA_TRY(cudaMemcpy(fcL_indx, c->t.idx, sizeof(short) * nxk * c->t.nD, kind));
   if (PC) HP_CUDA_TRY(cudaMemcpy(PC, c->t.PC, sizeof(double) * 3 * nR, kind));
@@ -289,7 +334,7 @@ extern "C" int hp_collision_df(hp_collision* c, const double* f, double* df, int
   if (!c || !f || !df) { hp_set_error("null argument"); return HP_ERR_INVALID; }
   if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("bad mem"); return HP_ERR_INVALID; }
   hp_plan* p = c->plan;
-  const long long nR = 8LL * p->B * p->B * p->B, nx = (long long)p->N * p->N, n = nR * nx;
+  const long long nR = 8LL * p->B * p->B * p->B, nx = p->nx, n = nR * nx;
   int st = HP_OK;
   const double* fd = f;
   double* dd = df;
@@ -389,7 +434,7 @@ template <typename T>
 static int coll_apply_T(hp_collision* c, T* f, double dt, cudaStream_t s) {
   hp_plan* p = c->plan;
   if (c->t.numR == 0) return HP_OK;
-  const long long nR = 8LL * p->B * p->B * p->B, nx = (long long)p->N * p->N, nt = nx * c->t.numR;
+  const long long nR = 8LL * p->B * p->B * p->B, nx = p->nx, nt = nx * c->t.numR;
   const int nD = c->t.nD;
   int st = HP_OK;
   if (!c->fcLT) {

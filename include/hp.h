@@ -214,7 +214,7 @@ int hp_pendulum_derivative_noalloc(hp_plan* plan, const double* F, double* dF);
 int hp_fftSO3_prod(hp_plan* plan, const double* F, const double* G, double* FG, int batch,
                    int mem);
 
-/* ---- hybrid collision operator (2-D reduced model, FP64) ----
+/* ---- hybrid collision operator (2-D reduced model and 3-D Omega, FP64 tables) ----
  * hp_collision_create builds the one-time tables of the reference's
  *   [lambda,indR,PC] = getLambda_mex(R,x,dWall,h,r,theta_t,lambda_max,false)
  *     (propagation/discrete/mex/sources/pendulum_reduced_collision/src/getLambda.cu:8-85)
@@ -227,7 +227,14 @@ int hp_fftSO3_prod(hp_plan* plan, const double* F, const double* G, double* FG, 
  *     (.../src/mexPropagate.cpp:6-77, propagate.cu:6-121; caller pendulum_reduced_hybrid.m:232)
  * with f, df real grid densities f(a,b,c,i,j).  hp_collision_tables copies the
  * tables out in the MEX layouts: lambda [ix][k], indR [k] (0-based), omega
- * [ix][k][2], fcL and fcL_indx [ix][k][d], PC [iR][3]; NULL skips a table. */
+ * [ix][k][ndim], fcL and fcL_indx [ix][k][d], PC [iR][3]; NULL skips a table.
+ * On a 3-D plan (no reference counterpart: getOmega.cu:86-96 takes
+ * Omega = [x1, x2, 0]) the operator uses all three components: omega = R Omega
+ * in the switching rate and the reset map, Omega+ in R^3 and a 3-D Gaussian
+ * landing kernel of covariance Gd (3x3); ix = i + 2Bx j + 4Bx^2 k, at most
+ * 32768 omega points (16-bit tap indices).  hp_state_hybrid_step accepts
+ * a coefficient-gravity model (hp_plan_set_model) as well as the density-
+ * gravity model, so a 3-D plan runs the 3-D hybrid loop. */
 typedef struct hp_collision hp_collision;
 typedef struct {
   double d, h, r;          /* wall distance, pivot-to-tip height, tip radius */
@@ -235,7 +242,8 @@ typedef struct {
   double lambda_max;       /* maximum switching rate                       */
   double epsilon;          /* coefficient of restitution                   */
   double L;                /* omega-grid period                            */
-  double Gd[4];            /* reset-noise covariance, column-major 2x2     */
+  double Gd[9];            /* reset-noise covariance, column-major ndim x ndim
+                              in the first ndim^2 entries                  */
   int nD;                  /* taps kept per landing point (<= 32)          */
 } hp_collision_params;
 int hp_collision_create(hp_plan* plan, const hp_collision_params* params, hp_collision** coll, int* numR);
@@ -307,8 +315,11 @@ int hp_state_step(hp_state* state, double dt, int method, int nsteps);
  *   F = propagate_den(F, f); f = fftSO3R backward(F); f += dt*df(f); F = forward(f)
  * with df the collision operator of `coll` (pendulum_reduced_discrete_propagate,
  * propagation/discrete/mex/sources/pendulum_reduced_collision/propagate.cu:6-121).
- * The plan needs hp_plan_set_den_model; coll must be created on the same plan.
- * The grid density f stays on the device between steps (compute precision). */
+ * The plan needs a model: the density-gravity model of hp_plan_set_den_model
+ * (the reference's hybrid loop), or a coefficient-gravity model of
+ * hp_plan_set_model (then F = propagate(F), e.g. the 3-D pendulum with the
+ * 3-D collision operator); coll must be created on the same plan.  The grid
+ * density f stays on the device between steps (compute precision). */
 int hp_state_hybrid_step(hp_state* state, hp_collision* coll, double dt, int method, int nsteps);
 /* Density on the grid of the current state into `f` (device pointer; double
  * for HP_FP64 plans, float for HP_MIXED plans): after hybrid steps the

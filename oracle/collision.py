@@ -8,8 +8,9 @@ Thrust and cannot be built or run here).
 Arrays follow the MEX layouts:
   R       (2B, 2B, 2B, 3, 3) rotations, grid index iR = a + 2B b + 4B^2 c
   x       (2, 2Bx, 2Bx) grid, point index ix = i + 2Bx j
+          (3-D Omega: (3, 2Bx, 2Bx, 2Bx), ix = i + 2Bx j + 4Bx^2 k)
   lambda  [ix][k]  (numR fastest), k indexes the colliding attitudes indR
-  Omega   [ix][k][2]
+  Omega   [ix][k][ndim]
   fcL, fcL_indx  [ix][k][d] (nD fastest)
   f, df   [ix][iR]  (the density f(a, b, c, i, j) in column-major order)
 """
@@ -27,8 +28,8 @@ def _rows(R):
 
 
 def _xpts(x):
-    """x (2, N, N) as (nx, 2) in point order i + N j."""
-    return np.transpose(x, (2, 1, 0)).reshape(-1, 2)
+    """x (nd, N, ...) as (nx, nd) in point order i + N j (+ N^2 k)."""
+    return x.T.reshape(-1, x.shape[0])
 
 
 def get_lambda(R, x, d, h, r, theta_t, lambda_max):
@@ -45,9 +46,11 @@ def get_lambda(R, x, d, h, r, theta_t, lambda_max):
                     lambda_max / 2 * np.sin(math.pi / (2 * theta_t) * (theta - theta0)) + lambda_max / 2)
     lam0 = np.where(cat == 0, 0.0, lam0)[indR]
     X = _xpts(x)
+    nd = X.shape[1]
     Rk = Rr[indR]                                                   # (numR, 3, 3)
-    om0 = Rk[None, :, 1, 0] * X[:, None, 0] + Rk[None, :, 1, 1] * X[:, None, 1]
-    om1 = Rk[None, :, 2, 0] * X[:, None, 0] + Rk[None, :, 2, 1] * X[:, None, 1]
+    # omega = R Omega with Omega = [x1, x2, 0] (2-D) or [x1, x2, x3] (3-D)
+    om0 = np.einsum('kj,xj->xk', Rk[:, 1, :nd], X)
+    om1 = np.einsum('kj,xj->xk', Rk[:, 2, :nd], X)
     vC = om0 * PC[indR][None, :, 2] - om1 * PC[indR][None, :, 1]
     lam = np.where(vC < 0.0, 0.0, np.broadcast_to(lam0[None, :], vC.shape))
     return lam, indR, PC
@@ -56,18 +59,19 @@ def get_lambda(R, x, d, h, r, theta_t, lambda_max):
 def get_omega_new(R, x, indR, epsilon):
     """getOmega(..., 'new') (getOmega.cu:64-103): post-collision angular velocity
     Omega+ = R^T(w - (1+eps)(w.t) t), w = R [x1, x2, 0], t = (R33, -R23)/|.| in
-    the (2, 3) components."""
+    the (2, 3) components, first ndim components kept.  For a 3-D grid (no
+    reference counterpart) w = R [x1, x2, x3] and Omega+ keeps all three."""
     Rk = _rows(R)[indR]
     X = _xpts(x)
+    nd = X.shape[1]
     n = np.sqrt(Rk[:, 1, 2] ** 2 + Rk[:, 2, 2] ** 2)
     t1, t2 = Rk[:, 2, 2] / n, -Rk[:, 1, 2] / n
-    w = np.einsum('kij,xj->xki', Rk[:, :, :2], X)                    # (nx, numR, 3)
+    w = np.einsum('kij,xj->xki', Rk[:, :, :nd], X)                   # (nx, numR, 3)
     ot = (1.0 + epsilon) * (w[..., 1] * t1 + w[..., 2] * t2)
     w1 = w[..., 1] - ot * t1
     w2 = w[..., 2] - ot * t2
-    O0 = Rk[None, :, 0, 0] * w[..., 0] + Rk[None, :, 1, 0] * w1 + Rk[None, :, 2, 0] * w2
-    O1 = Rk[None, :, 0, 1] * w[..., 0] + Rk[None, :, 1, 1] * w1 + Rk[None, :, 2, 1] * w2
-    return np.stack([O0, O1], -1)
+    return np.stack([Rk[None, :, 0, c] * w[..., 0] + Rk[None, :, 1, c] * w1 + Rk[None, :, 2, c] * w2
+                     for c in range(nd)], -1)
 
 
 def get_fcL(x, Omega, lam, Gd, nD):
@@ -77,18 +81,23 @@ def get_fcL(x, Omega, lam, Gd, nD):
     sort), normalise per source point over the kept taps (times dx^2), then scale
     by lambda(k, ix2) dx^2.  Returns fcL, fcL_indx as [ix1][k][d]."""
     X = _xpts(x)
+    nd = X.shape[1]
     nx, numR = Omega.shape[0], Omega.shape[1]
-    Gd = np.asarray(Gd, float).reshape(2, 2, order='F')
-    det = Gd[0, 0] * Gd[1, 1] - Gd[0, 1] * Gd[1, 0]
-    cn = 1 / (2 * math.pi * math.sqrt(det))
-    inv = np.array([[Gd[1, 1], -Gd[0, 1]], [-Gd[1, 0], Gd[0, 0]]]) / det
-    dx2 = (X[1, 0] - X[0, 0]) ** 2
+    Gd = np.asarray(Gd, float).reshape(nd, nd, order='F')
+    det = np.linalg.det(Gd) if nd == 3 else Gd[0, 0] * Gd[1, 1] - Gd[0, 1] * Gd[1, 0]
+    cn = 1 / ((2 * math.pi) ** (nd / 2) * math.sqrt(det))
+    inv = (np.linalg.inv(Gd) if nd == 3
+           else np.array([[Gd[1, 1], -Gd[0, 1]], [-Gd[1, 0], Gd[0, 0]]]) / det)
+    dx2 = (X[1, 0] - X[0, 0]) ** nd
     fcL = np.zeros((nx, numR, nD))
     idx = np.zeros((nx, numR, nD), np.int16)
     for k in range(numR):
-        dO = X[:, None, :] - Omega[None, :, k, :]                   # (ix1, ix2, 2)
+        dO = X[:, None, :] - Omega[None, :, k, :]                   # (ix1, ix2, nd)
         q = (inv[0, 0] * dO[..., 0] ** 2 + (inv[0, 1] + inv[1, 0]) * dO[..., 0] * dO[..., 1]
              + inv[1, 1] * dO[..., 1] ** 2)
+        if nd == 3:
+            q = q + ((inv[0, 2] + inv[2, 0]) * dO[..., 0] * dO[..., 2]
+                     + (inv[1, 2] + inv[2, 1]) * dO[..., 1] * dO[..., 2] + inv[2, 2] * dO[..., 2] ** 2)
         fc = np.exp(-0.5 * q) * cn                                  # (ix1, ix2)
         order = np.argsort(-fc, axis=1, kind='stable')[:, :nD]
         vals = np.take_along_axis(fc, order, 1)

@@ -89,12 +89,52 @@ def test_hybrid_steps_vs_oracle(hp, B, Bx, precision, method):
     assert rel(fg, fref) < tol
 
 
-def test_hybrid_needs_den_model(hp):
+def test_hybrid_needs_a_model(hp):
     B, Bx = 3, 2
     P = pd.pendulum_reduced(B, Bx, L=3.4)
     plan = hp.Plan(B, Bx, 2, 0, hp.HP_REAL)
-    plan.set_model(P.L, P.b, P.G, P.MR)
     coll = hp.Collision(plan, L=P.L, Gd=0.0025 * np.eye(2), nD=4, **PRM)
     st = hp.State(plan)
     with pytest.raises(hp.HPError):
         st.hybrid_step(coll, 0.01, 'euler', 1)
+
+
+def oracle_hybrid_cg(F, P, t, dt, method, nsteps):
+    """Hybrid loop with the coefficient-gravity derivative (any ndim)."""
+    for _ in range(nsteps):
+        F = pd.integrate(F, lambda Fx: pd.derivative_fast(Fx, P), dt, method)
+        fg = np.real(so3.ifftSO3R_backward(F, real=True))
+        nR = fg.shape[0] * fg.shape[1] * fg.shape[2]
+        fl = fg.T.reshape(-1, nR)
+        fl = fl + dt * co.propagate_noise(fl, t['lambda_'], t['indR'], t['fcL'], t['fcL_indx'])
+        F = so3.fftSO3R_forward(fl.reshape(fg.T.shape).T)
+    return F
+
+
+@pytest.mark.parametrize('ndim,B,Bx', [(2, 4, 3), (3, 4, 3)])
+@pytest.mark.parametrize('precision', [0, 1])
+def test_hybrid_coefficient_model(hp, ndim, B, Bx, precision):
+    """Hybrid steps with a coefficient-gravity model: the reduced pendulum with
+    Clebsch-Gordan gravity, and the 3-D pendulum with the 3-D collision operator."""
+    P = pd.pendulum_3d(B, Bx, L=4.0) if ndim == 3 else pd.pendulum_reduced(B, Bx, L=3.4)
+    f0, _ = pd.seeded_density(B, Bx, ndim, P.L, seed=B + ndim, sigma=0.5)
+    F0 = so3.fftSO3R_forward(f0)
+    Gd = 0.0025 * np.eye(ndim)
+    dt = 0.005
+    plan = hp.Plan(B, Bx, ndim, precision, hp.HP_REAL)
+    gyro = (0.0, 0.0, 0.0)
+    if ndim == 3:
+        J = np.diag(P.params['J'])
+        gyro = ((J[1] - J[2]) / J[0], (J[2] - J[0]) / J[1], (J[0] - J[1]) / J[2])
+    plan.set_model(P.L, P.b, P.G, P.MR, gyro)
+    coll = hp.Collision(plan, L=P.L, Gd=Gd, nD=8, **PRM)
+    assert coll.numR > 0
+    Fref = oracle_hybrid_cg(F0, P, coll.tables(), dt, 'RK2', 2)
+    st = hp.State(plan)
+    st.load(F0)
+    st.hybrid_step(coll, dt, 'RK2', 2)
+    F = st.store()
+    if precision == 0:
+        assert rel(F - F0, Fref - F0) < 1e-10
+    else:
+        assert rel(F, Fref) < 1e-6
