@@ -84,12 +84,17 @@ __global__ void k_coll_lambda_omega(int B, int N, double L, int numR, const int*
   const double x3 = NDIM == 3 ? -L / 2 + L / N * (ix / (N * N)) : 0.0;
   double lam = cat[iR] == 2 ? lmax : lmax / 2 * sin(M_PI / (2 * thetat) * (theta[iR] - theta0)) + lmax / 2;
   if (cat[iR] == 0) lam = 0.0;
-  // omega = R Omega (spatial angular velocity); contact-point velocity along the wall normal
-  const double w0 = R[0][0] * x1 + R[0][1] * x2 + R[0][2] * x3;
-  double w1 = R[1][0] * x1 + R[1][1] * x2 + R[1][2] * x3;
-  double w2 = R[2][0] * x1 + R[2][1] * x2 + R[2][2] * x3;
-  const double vC = w1 * PC[3 * iR + 2] - w2 * PC[3 * iR + 1];
+  // omega = R Omega (spatial angular velocity); contact-point velocity along
+  // the wall normal, (omega x PC)_1.  PC's (2, 3) components are lr3 R e3's, so
+  // the spin x3 R e3 about the pendulum axis drops out exactly: the velocity
+  // is formed from x1, x2 alone, as in the 2-D model (with x3 it would be
+  // rounding noise at x1 = x2 = 0, whose sign would pick lambda).
+  const double v1 = R[1][0] * x1 + R[1][1] * x2, v2 = R[2][0] * x1 + R[2][1] * x2;
+  const double vC = v1 * PC[3 * iR + 2] - v2 * PC[3 * iR + 1];
   lambda[t] = vC < 0.0 ? 0.0 : lam;
+  const double w0 = R[0][0] * x1 + R[0][1] * x2 + R[0][2] * x3;
+  double w1 = v1 + R[1][2] * x3;
+  double w2 = v2 + R[2][2] * x3;
   // reset map
   const double nt = sqrt(R[1][2] * R[1][2] + R[2][2] * R[2][2]);
   const double t1 = R[2][2] / nt, t2 = -R[1][2] / nt;
@@ -158,7 +163,9 @@ __global__ void k_coll_scale(int nx, int numR, int nD, double dxn, const double*
   if (t >= (long long)nx * numR * nD) return;
   const int k = (int)((t / nD) % numR);
   const long long src = (long long)idx[t] * numR + k;
-  fcL[t] = fcL[t] / (norm[src] * dxn) * (lambda[src] * dxn);
+  // a source whose every kept tap underflowed to 0 has norm 0: its taps stay 0
+  // (the reference divides unguarded; its 2-D setups never reach 0/0)
+  fcL[t] = norm[src] > 0.0 ? fcL[t] / (norm[src] * dxn) * (lambda[src] * dxn) : 0.0;
 }
 
 // df(R_k, x) = sum_d fcL f(R_k, idx) - lambda f(R_k, x); rows of non-colliding

@@ -46,11 +46,12 @@ def get_lambda(R, x, d, h, r, theta_t, lambda_max):
                     lambda_max / 2 * np.sin(math.pi / (2 * theta_t) * (theta - theta0)) + lambda_max / 2)
     lam0 = np.where(cat == 0, 0.0, lam0)[indR]
     X = _xpts(x)
-    nd = X.shape[1]
     Rk = Rr[indR]                                                   # (numR, 3, 3)
-    # omega = R Omega with Omega = [x1, x2, 0] (2-D) or [x1, x2, x3] (3-D)
-    om0 = np.einsum('kj,xj->xk', Rk[:, 1, :nd], X)
-    om1 = np.einsum('kj,xj->xk', Rk[:, 2, :nd], X)
+    # omega = R Omega with Omega = [x1, x2, 0] (2-D).  On a 3-D grid the spin x3
+    # R e3 about the pendulum axis adds nothing to (omega x PC)_1 (PC's (2, 3)
+    # components are lr3 R e3's), so the contact velocity uses x1, x2 alone.
+    om0 = Rk[None, :, 1, 0] * X[:, None, 0] + Rk[None, :, 1, 1] * X[:, None, 1]
+    om1 = Rk[None, :, 2, 0] * X[:, None, 0] + Rk[None, :, 2, 1] * X[:, None, 1]
     vC = om0 * PC[indR][None, :, 2] - om1 * PC[indR][None, :, 1]
     lam = np.where(vC < 0.0, 0.0, np.broadcast_to(lam0[None, :], vC.shape))
     return lam, indR, PC
@@ -104,7 +105,8 @@ def get_fcL(x, Omega, lam, Gd, nD):
         norm = np.zeros(nx)
         np.add.at(norm, order.ravel(), vals.ravel())
         norm *= dx2
-        vals = vals / norm[order]
+        nz = norm[order] > 0          # 0/0 (every kept tap of a source underflowed) -> 0
+        vals = np.where(nz, vals / np.where(nz, norm[order], 1.0), 0.0)
         vals = vals * lam[order, k] * dx2
         fcL[:, k, :] = vals
         idx[:, k, :] = order

@@ -119,7 +119,7 @@ def test_hybrid_coefficient_model(hp, ndim, B, Bx, precision):
     P = pd.pendulum_3d(B, Bx, L=4.0) if ndim == 3 else pd.pendulum_reduced(B, Bx, L=3.4)
     f0, _ = pd.seeded_density(B, Bx, ndim, P.L, seed=B + ndim, sigma=0.5)
     F0 = so3.fftSO3R_forward(f0)
-    Gd = 0.0025 * np.eye(ndim)
+    Gd = (0.0025 if ndim == 2 else 0.04) * np.eye(ndim)
     dt = 0.005
     plan = hp.Plan(B, Bx, ndim, precision, hp.HP_REAL)
     gyro = (0.0, 0.0, 0.0)

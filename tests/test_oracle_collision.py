@@ -68,3 +68,50 @@ def test_reset_map_restitution_and_momentum():
     assert abs(vC_new[0] + eps * vC_o[0]) < 1e-12
     # omega+ - omega is parallel to t, and t is parallel to (PC x e1) projected:
     assert np.linalg.norm(np.cross(omega_new - omega_old, t)) < 1e-12
+
+
+def test_3d_omega_extension_properties():
+    """The 3-D Omega extension: lambda does not depend on the spin x3 about the
+    pendulum axis; with x3 = 0 the reset map equals the 2-D one; the reset
+    leaves the axial spin's contribution to omega unchanged."""
+    B, Bx, L = 4, 3, 3.4
+    R = so3.rotation_grid(B)
+    x2 = pd.omega_grid(Bx, L, 2)
+    x3 = pd.omega_grid(Bx, L, 3)
+    a = (PARAMS['d'], PARAMS['h'], PARAMS['r'], PARAMS['theta_t'], PARAMS['lambda_max'])
+    lam2, ind2, _ = co.get_lambda(R, x2, *a)
+    lam3, ind3, _ = co.get_lambda(R, x3, *a)
+    N = 2 * Bx
+    assert np.array_equal(ind2, ind3)
+    lam3 = lam3.reshape(N, N * N, -1)                 # [k3][i + N j][k]
+    for k3 in range(N):
+        assert np.array_equal(lam3[k3], lam2)
+    Om2 = co.get_omega_new(R, x2, ind2, PARAMS['epsilon'])
+    Om3 = co.get_omega_new(R, x3, ind3, PARAMS['epsilon']).reshape(N, N * N, len(ind3), 3)
+    z = N // 2                                         # x3 = 0 plane
+    assert np.abs(Om3[z, :, :, :2] - Om2).max() < 1e-13
+    # a spin-only state (x1 = x2 = 0) is not reset: Omega+ = Omega
+    c = N // 2
+    spin = Om3[:, c + N * c, :, :]                     # x1 = x2 = 0, every x3
+    xs = -L / 2 + L / N * np.arange(N)
+    assert np.abs(spin[:, :, 2] - xs[:, None]).max() < 1e-12
+    assert np.abs(spin[:, :, :2]).max() < 1e-12
+
+
+def test_3d_fcl_never_nan_and_normalised():
+    """A narrow 3-D landing kernel underflows at far landing points: those taps
+    are 0 (no 0/0), and every source that keeps a tap still loses exactly lambda."""
+    B, Bx, L = 4, 3, 4.0
+    R = so3.rotation_grid(B)
+    x = pd.omega_grid(Bx, L, 3)
+    lam, indR, _ = co.get_lambda(R, x, PARAMS['d'], PARAMS['h'], PARAMS['r'], PARAMS['theta_t'],
+                                 PARAMS['lambda_max'])
+    Om = co.get_omega_new(R, x, indR, PARAMS['epsilon'])
+    fcL, idx = co.get_fcL(x, Om, lam, (0.0025 * np.eye(3)).ravel(order='F'), 8)
+    assert np.isfinite(fcL).all()
+    nx, k = lam.shape
+    out = np.zeros((nx, k))
+    for d in range(8):
+        np.add.at(out, (idx[:, :, d].astype(np.int64), np.arange(k)[None, :]), fcL[:, :, d])
+    kept = out > 0
+    assert np.allclose(out[kept], lam[kept], rtol=1e-12)
