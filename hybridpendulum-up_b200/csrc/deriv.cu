@@ -41,9 +41,11 @@ using namespace hp;
 
 
 // -------------------------------------------------------- pass A: axis 3 ----
+// Fc (may be null): the coefficients themselves in the compute precision, the
+// input the local and plane passes then read instead of the FP64 state.
 template <int N, typename T>
 __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __restrict__ F,
-                                               c2<T>* __restrict__ P3, T Llen) {
+                                               c2<T>* __restrict__ P3, T Llen, c2<T>* __restrict__ Fc) {
   using C = c2<T>;
   constexpr long long plane = (long long)N * N;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -53,6 +55,11 @@ __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __res
   C x[N];
 #pragma unroll
   for (int j = 0; j < N; ++j) x[j] = cvt<C, double2>(__ldg(src + j * plane));
+  if (Fc) {
+    C* fc = Fc + row * L.nx + p;
+#pragma unroll
+    for (int j = 0; j < N; ++j) fc[j * plane] = x[j];
+  }
   fft<N, true>(x);
 #pragma unroll
   for (int j = 0; j < N; ++j) {
@@ -77,8 +84,8 @@ template <typename T> __host__ __device__ constexpr size_t local_tile_bytes(int 
   return ((size_t)rmax * W * sizeof(c2<T>) + 15) / 16 * 16;
 }
 
-template <typename T, int W, int NDIM>
-__global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __restrict__ F,
+template <typename T, int W, int NDIM, typename TIN>
+__global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __restrict__ F,
                                                c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
                                                const c2<T>* __restrict__ Gx, const c2<T>* __restrict__ sdk,
                                                DerivParams prm) {
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const double2* __res
     for (int u = 0; u < 8; ++u) {
       const int e = e0 + u * nth;
       const int r = e / W, w = e % W;
-      v[u] = (e < R * W && w0 + w < L.nx) ? cvt<C, double2>(F[(size_t)(r0 + r) * L.nx + w0 + w]) : czero<C>();
+      v[u] = (e < R * W && w0 + w < L.nx) ? cvt<C, c2<TIN>>(F[(size_t)(r0 + r) * L.nx + w0 + w]) : czero<C>();
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -229,9 +236,9 @@ __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, in
 //   [C+2, 2C+2)        P~ rows n0 .. n0+C-1     (ndim = 3)
 //   [2C+2, 3C+2)       A  = FFT2(Y0) + D_2 FFT2(Y2), then FFT_1
 //   [3C+2, 4C+2)       Y1' = FFT_2(Y1), then D_1 FFT_1
-template <int N, typename T, bool HAS_P3>
+template <int N, typename T, bool HAS_P3, typename TIN>
 __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
-                                                  const double2* __restrict__ Fev,
+                                                  const c2<TIN>* __restrict__ Fev,
                                                   const c2<T>* __restrict__ P3,
                                                   const c2<T>* __restrict__ Gl,
                                                   const double2* __restrict__ F0, double a,
@@ -272,7 +279,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
         if (e < tot) {
           const int sl = e / (N * N), q = e % (N * N);
           const int n = tl.n0 - 1 + sl;
-          if (n >= -tl.l && n <= tl.l) v[u] = cvt<C, double2>(Fev[row_of(L, tl.l, tl.m, n) * L.nx + pbase + q]);
+          if (n >= -tl.l && n <= tl.l) v[u] = cvt<C, c2<TIN>>(Fev[row_of(L, tl.l, tl.m, n) * L.nx + pbase + q]);
         }
       }
 #pragma unroll
@@ -495,31 +502,31 @@ template <typename T> static size_t plane_smem(int N, bool p3) {
 
 // k_local with the widest omega tile (32/16/8/4 points) whose group tile and
 // tap weights fit 110 KB of shared memory (the m = 0 group has (lmax+1)^2 rows).
-template <typename T, int W>
-static int local_w_launch(hp_plan* p, const double2* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
+template <typename T, int W, typename TIN>
+static int local_w_launch(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
                           cudaStream_t s) {
   const size_t lsm = local_smem<T>(p, W);
   dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
   ProfScope _ps(p, "deriv.local", s);
   if (p->ndim == 3) {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 3><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   } else {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 2><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
 
-template <typename T>
-static int launch_local(hp_plan* p, const double2* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
+template <typename T, typename TIN = double>
+static int launch_local(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
                         cudaStream_t s) {
   constexpr size_t budget = 110 * 1024;
-  if (sizeof(T) == 4 && local_smem<T>(p, 32) <= budget) return local_w_launch<T, 32>(p, F, G, Gx, prm, s);
-  if (local_smem<T>(p, 16) <= budget) return local_w_launch<T, 16>(p, F, G, Gx, prm, s);
-  if (local_smem<T>(p, 8) <= budget) return local_w_launch<T, 8>(p, F, G, Gx, prm, s);
-  if (local_smem<T>(p, 4) <= (size_t)200 * 1024) return local_w_launch<T, 4>(p, F, G, Gx, prm, s);
+  if (sizeof(T) == 4 && local_smem<T>(p, 32) <= budget) return local_w_launch<T, 32, TIN>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 16) <= budget) return local_w_launch<T, 16, TIN>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 8) <= budget) return local_w_launch<T, 8, TIN>(p, F, G, Gx, prm, s);
+  if (local_smem<T>(p, 4) <= (size_t)200 * 1024) return local_w_launch<T, 4, TIN>(p, F, G, Gx, prm, s);
   hp_set_error("gravity pass tiles exceed shared memory for this bandlimit");
   return HP_ERR_UNSUPPORTED;
 }
@@ -537,14 +544,27 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   }
   C* G = (C*)p->ws_get("deriv.G", fb, &st);
   if (st) return st;
+  // mixed 3-D plans: the axis-3 pass also leaves F in FP32 (Fc), which the
+  // local and plane passes read in place of the FP64 state (the values they
+  // convert to anyway), halving their coefficient traffic
+  C* Fc = nullptr;
+  if (p->ndim == 3 && sizeof(T) == 4) {
+    Fc = (C*)p->ws_get("deriv.F32", fb, &st);
+    if (st) return st;
+  }
   const RowLayout L = p->layout();
   if (p->ndim == 3) {
     const long long nt = p->nrows * (long long)N * N;
     ProfScope _ps(p, "deriv.axis3", s);
-    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L);
+    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L, Fc);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  ST_CHECK(launch_local<T>(p, Fev, G, (const C*)Gx, prm, s));
+  if (Fc) {
+    st = launch_local<T, T>(p, Fc, G, (const C*)Gx, prm, s);
+  } else {
+    st = launch_local<T>(p, Fev, G, (const C*)Gx, prm, s);
+  }
+  if (st) return st;
   // tiles: every (m, l) row split into chunks of CT consecutive n (built once per plan)
   constexpr int CT = PlaneCfg<T>::C;
   const char tkey[] = {'d', 'e', 'r', 'i', 'v', '.', 't', 'i', 'l', 'e', 's', (char)('0' + CT), 0};
@@ -563,12 +583,15 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)htiles.size(), p3 ? N : 1);
   ProfScope _ps(p, "deriv.plane", s);
-  if (p3) {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+  if (p3 && Fc) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, true, T><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fc, P3, G, F0, a, out, acc, bacc, prm);
+  } else if (p3) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, true, double><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   } else {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, false, double><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
@@ -848,18 +871,18 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   HP_CUDA_TRY(cudaGetLastError());
   if (p3) {
     const long long nt = p->nrows * (long long)N * N;
-    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fi, P3, (T)prm.L);
+    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fi, P3, (T)prm.L, (c2<T>*)nullptr);
     HP_CUDA_TRY(cudaGetLastError());
   }
   ST_CHECK(launch_local<T>(p, Fi, G, (const c2<T>*)nullptr, prm, s));
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)ntiles, p3 ? N : 1);
   if (p3) {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, true, double><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   } else {
-    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, false><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane<N, T, false, double><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, tiles, Fi, P3, G, nullptr, 1.0, dFi, nullptr, 0.0, prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return hp_internal_to_full(p, dFi, dFfull, s);

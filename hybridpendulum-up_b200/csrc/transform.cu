@@ -102,6 +102,27 @@ __device__ __forceinline__ void store16(double* dst, const double* s) {
 }
 
 // ------------------------------------------------------------ synthesis ----
+// Real staging of the synthesis: one run of NB*2B values per (omega point p,
+// gamma column c), runs RS elements apart.  FP32: RS = 4 (mod 32), and
+// element i of run (p, c) sits at (i & ~3) | ((i + p) & 3), a rotation by p
+// inside its 16-byte chunk.  The alpha-stage writers (lanes: p fastest, then
+// c) then hit 32 distinct banks per scalar store, and the store loop reads
+// whole 16-byte chunks (LDS.128, rotated back in registers).  FP64: runs
+// padded by one element, no rotation.
+template <typename T, int NB, int NB2> __host__ __device__ constexpr int synth_rs() {
+  return sizeof(T) == 4 ? (NB * NB2 + 27) / 32 * 32 + 4 : NB * NB2 + 1;
+}
+__device__ __forceinline__ int synth_swz(int i, int rot) { return (i & ~3) | ((i + rot) & 3); }
+// logical chunk from a physical one whose element k sits at (k + rot) & 3
+__device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
+  switch (rot & 3) {
+    case 0: return v;
+    case 1: return make_float4(v.y, v.z, v.w, v.x);
+    case 2: return make_float4(v.z, v.w, v.x, v.y);
+    default: return make_float4(v.w, v.x, v.y, v.z);
+  }
+}
+
 // Block = (group of NB consecutive beta indices, range of omega points), the
 // (2l+1)-weighted d values of its betas resident in shared memory.  Input rows
 // are read in the [row][omega] layout with the P omega points of a batch on
@@ -122,10 +143,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   // G/H stride per (bb, m): 2B q-bins x P omega points, padded by P so that
   // the P-wide groups of the gamma stage fall on distinct banks
   constexpr int GS = NB2 * P + P;
-  // real staging: runs of NB*2B values in slots of RS elements (a multiple of
-  // the RSB elements that span the 32 banks)
-  constexpr int RSB = 128 / (int)sizeof(T);
-  constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
+  constexpr int RS = synth_rs<T, NB, NB2>();
+  constexpr bool SWZ = sizeof(T) == 4;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nrows = (int)L.nrows;
   T* sds = reinterpret_cast<T*>(smraw);
@@ -249,14 +268,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
       } else {
-        // runs of NB*2B values per (p, c) padded by one element
-        constexpr int RS1 = NB * NB2 + 1;
-        T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS1 + bb * NB2;
-        T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS1 + bb * NB2;
+        T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS;
+        T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS;
+        const int rot = SWZ ? (p & 3) : 0;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) {
-          st[a] = x[a].x;
-          st2[a] = x[a].y;
+          const int i = bb * NB2 + a;
+          const int j = SWZ ? synth_swz(i, rot) : i;
+          st[j] = x[a].x;
+          st2[j] = x[a].y;
         }
       }
     }
@@ -276,12 +296,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
         for (int o = lane; o < nbv * NB2; o += 32) dst[o] = src[o];
       } else {
         T* dst = reinterpret_cast<T*>(fout) + gi;
-        const T* src = reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * (RUN + 1);
+        const T* src = reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * RS;
+        const int rot = SWZ ? (pp & 3) : 0;
         constexpr int VW = 16 / sizeof(T);   // elements per 16-byte vector
         if (nbv == NB && (RUN % VW) == 0 && (gi % VW) == 0) {
-          for (int o = lane * VW; o < RUN; o += 32 * VW) store16(dst + o, src + o);
+          if constexpr (SWZ) {
+            for (int o = lane * 4; o < RUN; o += 128)
+              *reinterpret_cast<float4*>(dst + o) = unrotate4(*reinterpret_cast<const float4*>(src + o), rot);
+          } else {
+            for (int o = lane * VW; o < RUN; o += 32 * VW) store16(dst + o, src + o);
+          }
         } else {
-          for (int o = lane; o < nbv * NB2; o += 32) dst[o] = src[o];
+          for (int o = lane; o < nbv * NB2; o += 32) dst[o] = src[SWZ ? synth_swz(o, rot) : o];
         }
       }
     }
@@ -363,8 +389,8 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr long long bytes(int nb, int p) {
     const long long c = 2 * (long long)sizeof(T);
     const long long g = (long long)nb * NM * (2 * B * p + p) * c;                     // G/H, padded
-    const long long rsb = 128 / (long long)sizeof(T);
-    const long long rs = ((long long)nb * 2 * B + rsb - 1) / rsb * rsb + 1;
+    const long long rs = sizeof(T) == 4 ? ((long long)nb * 2 * B + 27) / 32 * 32 + 4   // synth_rs
+                                        : (long long)nb * 2 * B + 1;
     const long long st = CPLX ? (long long)p * 2 * B * nb * 2 * B * c                 // f staging
                               : (long long)p * 2 * B * rs * (long long)sizeof(T);
     return (GD ? 0 : nb * nrows * (long long)sizeof(T)) + 32 + (long long)NM * (2 * B - 1) * 8 + (g > st ? g : st);
@@ -440,8 +466,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   constexpr bool GD = Cfg::GD;
   static_assert(NB * Cfg::NCOL * P <= 256, "alpha stage must fit one round");
   const size_t sd_bytes = GD ? 0 : ((size_t)NB * p->nrows * sizeof(T) + 15) / 16 * 16;
-  constexpr int RSB = 128 / (int)sizeof(T);
-  constexpr int RS = (NB * NB2 + RSB - 1) / RSB * RSB + 1;
+  constexpr int RS = synth_rs<T, NB, NB2>();
   const size_t sg_bytes = std::max((size_t)NB * NM * (NB2 * P + P) * sizeof(C),
                                    CPLX ? (size_t)P * NB2 * NB * NB2 * sizeof(C)
                                         : (size_t)P * NB2 * RS * sizeof(T));
