@@ -113,6 +113,20 @@ template <typename T, int NB, int NB2> __host__ __device__ constexpr int synth_r
   return sizeof(T) == 4 ? (NB * NB2 + 27) / 32 * 32 + 4 : NB * NB2 + 1;
 }
 __device__ __forceinline__ int synth_swz(int i, int rot) { return (i & ~3) | ((i + rot) & 3); }
+// Bulk (TMA engine) copy of a contiguous shared-memory run to global memory:
+// both addresses 16-byte aligned, size a multiple of 16 bytes.  The issuing
+// thread later waits for the source to have been read (wait_group.read) before
+// the buffer is rewritten, and for completion (wait_group) before exit.
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, unsigned bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(ssrc);
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(s), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// orders this thread's shared-memory writes before later bulk-copy reads of them
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 // logical chunk from a physical one whose element k sits at (k + rot) & 3
 __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
   switch (rot & 3) {
@@ -144,7 +158,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   // the P-wide groups of the gamma stage fall on distinct banks
   constexpr int GS = NB2 * P + P;
   constexpr int RS = synth_rs<T, NB, NB2>();
-  constexpr bool SWZ = sizeof(T) == 4;
+  // FP32 real plans with an even NB: every run (NB*2B or the last group's
+  // nbv*2B floats) starts 16-byte aligned in f and in the staging buffer, so
+  // the runs leave by bulk copies that drain while the next batch computes.
+  // Otherwise FP32 uses the rotated staging and vector stores.
+  constexpr bool BULK = sizeof(T) == 4 && !CPLX && NB % 2 == 0;
+  constexpr bool SWZ = sizeof(T) == 4 && !BULK;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nrows = (int)L.nrows;
   T* sds = reinterpret_cast<T*>(smraw);
@@ -166,9 +185,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   }
   for (int e = tid; e < NPAIR; e += nth) spairs[e] = pairs[e];
   const long long nx = L.nx;
+  // vector and bulk stores need a 16-byte aligned density buffer
+  const bool fout_al16 = (reinterpret_cast<unsigned long long>(fout) & 15ull) == 0;
   for (int bt = 0; bt < nbatch; ++bt) {
     const long long w0 = ((long long)chunk * nbatch + bt) * P;
     if (w0 >= nx) break;
+    if (BULK && fout_al16) bulk_wait_read_all();   // the previous batch's runs have left the staging (aliases sG)
     __syncthreads();
     // beta stage: item (pair, p), p fastest.  Pairs come from the block's copy
     // of the pair table (longest l-runs first, so the lanes of a warp run
@@ -280,12 +302,23 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
         }
       }
     }
+    if (BULK && fout_al16) fence_proxy_async_smem();
     __syncthreads();
     // store: f[a + 2B (b + 2B (c + 2B w))]; the nbv*2B values of one (w, c) are
     // contiguous in f and in the staging buffer; a warp copies one run with
     // consecutive lanes on consecutive 16-byte pieces.
     const int pc = (int)min((long long)P, nx - w0);
     constexpr int RUN = NB * NB2;
+    if (BULK && fout_al16) {
+      for (int run = tid; run < pc * NB2; run += nth) {
+        const int pp = run / NB2, cc = run % NB2;
+        const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2;
+        bulk_s2g(reinterpret_cast<T*>(fout) + gi, reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * RS,
+                 (unsigned)(nbv * NB2 * sizeof(T)));
+      }
+      bulk_commit();
+      continue;
+    }
     const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     for (int run = warp; run < pc * NB2; run += nwarps) {
       const int pp = run / NB2, cc = run % NB2;
@@ -299,7 +332,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
         const T* src = reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * RS;
         const int rot = SWZ ? (pp & 3) : 0;
         constexpr int VW = 16 / sizeof(T);   // elements per 16-byte vector
-        if (nbv == NB && (RUN % VW) == 0 && (gi % VW) == 0) {
+        if (fout_al16 && nbv == NB && (RUN % VW) == 0 && (gi % VW) == 0) {
           if constexpr (SWZ) {
             for (int o = lane * 4; o < RUN; o += 128)
               *reinterpret_cast<float4*>(dst + o) = unrotate4(*reinterpret_cast<const float4*>(src + o), rot);
@@ -312,6 +345,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
       }
     }
   }
+  if (BULK && fout_al16) bulk_wait_all();   // shared memory must outlive the bulk copies reading it
 }
 
 // -------------------------------------------------------------- drivers ----

@@ -211,3 +211,27 @@ def test_errors(hp):
     with pytest.raises(hp.HPError) as e:
         plan.propagate(F, 1e-3)
     assert e.value.code == hp.HP_ERR_NO_MODEL
+
+
+@pytest.mark.parametrize('B,Bx', [(15, 2), (6, 3), (5, 2)])
+def test_density_store_paths_agree(hp, B, Bx):
+    """The mixed synthesis writes its runs by bulk copies (16-byte aligned
+    buffer, even beta groups) or by plain stores (any other buffer): a density
+    written one float past an aligned address equals the aligned one exactly,
+    and both match the oracle."""
+    import torch
+    F = random_coeffs(B, (2 * Bx,) * 3, seed=B + 1, hermitian=True)
+    ref = so3.ifftSO3R_backward(F, real=True)
+    plan = hp.Plan(B, Bx, 3, hp.HP_MIXED, hp.HP_REAL)
+    st = hp.State(plan)
+    st.load(F)
+    n = int(np.prod(plan.f_shape))
+    buf = torch.zeros(n + 4, dtype=torch.float32, device='cuda')
+    st.density_into(buf.data_ptr())
+    a = buf[:n].clone()
+    buf.zero_()
+    st.density_into(buf.data_ptr() + 4)          # one float off the 16-byte grid
+    torch.cuda.synchronize()
+    assert torch.equal(buf[1:n + 1], a) and float(buf[0]) == 0.0 and float(buf[n + 1:].abs().sum()) == 0.0
+    f = a.double().cpu().numpy().reshape(tuple(reversed(plan.f_shape))).transpose()
+    assert rel(f, ref) < TOLMIX
