@@ -89,6 +89,24 @@ __device__ __forceinline__ C twiddle(int e, int M) {
   return w;
 }
 
+// ------------------------------------------------ asynchronous smem fill ----
+// cp.async of one element (8 or 16 bytes) from global to shared memory without
+// a register round trip; src_bytes = 0 writes zeros (the source is not read).
+// Completion: cp_async_wait_all() by the issuing thread, then a block barrier.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool valid) {
+  static_assert(BYTES == 8 || BYTES == 16, "cp.async of 8 or 16 bytes");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int nb = valid ? BYTES : 0;
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(nb) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(nb) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // ------------------------------------------------- register-resident FFT ----
 // Small DFT of radix R in registers (out-of-place on v).
 template <int R, bool INV, typename C>
@@ -180,8 +198,59 @@ __device__ __forceinline__ void fft_stages(C (&x)[N]) {
   }
 }
 
+// 30 = 2 * 3 * 5 by the prime-factor (Good-Thomas) algorithm, no twiddles:
+// with n = (15 n1 + 10 n2 + 6 n3) mod 30 and k = (15 k1 + 10 k2 + 6 k3) mod 30,
+// nk = 15 n1k1 + 10 n2k2 + 6 n3k3 (mod 30), so the 30-point DFT is a 2 x 3 x 5
+// DFT over (n1, n2, n3) with both index maps applied as register permutations.
+template <bool INV, typename C>
+__device__ __forceinline__ void fft30_pfa(C (&x)[30]) {
+  C y[30];   // y[(n1 * 3 + n2) * 5 + n3] = x[(15 n1 + 10 n2 + 6 n3) % 30]
+#pragma unroll
+  for (int n1 = 0; n1 < 2; ++n1)
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2)
+#pragma unroll
+      for (int n3 = 0; n3 < 5; ++n3) y[(n1 * 3 + n2) * 5 + n3] = x[(15 * n1 + 10 * n2 + 6 * n3) % 30];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {   // length-5 DFTs along n3
+    C v[5];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) v[r] = y[a * 5 + r];
+    dft_small<5, INV>(v);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) y[a * 5 + r] = v[r];
+  }
+#pragma unroll
+  for (int n1 = 0; n1 < 2; ++n1)   // length-3 DFTs along n2
+#pragma unroll
+    for (int k3 = 0; k3 < 5; ++k3) {
+      C v[3];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) v[r] = y[(n1 * 3 + r) * 5 + k3];
+      dft_small<3, INV>(v);
+#pragma unroll
+      for (int r = 0; r < 3; ++r) y[(n1 * 3 + r) * 5 + k3] = v[r];
+    }
+#pragma unroll
+  for (int b = 0; b < 15; ++b) {   // length-2 DFTs along n1
+    C v[2] = {y[b], y[15 + b]};
+    dft_small<2, INV>(v);
+    y[b] = v[0];
+    y[15 + b] = v[1];
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 2; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 3; ++k2)
+#pragma unroll
+      for (int k3 = 0; k3 < 5; ++k3) x[(15 * k1 + 10 * k2 + 6 * k3) % 30] = y[(k1 * 3 + k2) * 5 + k3];
+}
+
 template <int N, bool INV, typename C>
-__device__ __forceinline__ void fft(C (&x)[N]) { fft_stages<N, 1, INV>(x); }
+__device__ __forceinline__ void fft(C (&x)[N]) {
+  if constexpr (N == 30) fft30_pfa<INV>(x);
+  else fft_stages<N, 1, INV>(x);
+}
 
 // Fourier index k (FFT order) -> signed wavenumber with the Nyquist bin zeroed
 // (the 2 pi i [0:Bx-1, 0, -Bx+1:-1] / L multiplier of the first derivative).

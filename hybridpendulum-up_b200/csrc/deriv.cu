@@ -97,13 +97,15 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
   T* sw = reinterpret_cast<T*>(smraw + local_tile_bytes<T>(rmax, W));             // [R][9]
   int* sseg = reinterpret_cast<int*>(smraw + local_tile_bytes<T>(rmax, W) +
                                      ((size_t)rmax * 9 * sizeof(T) + 15) / 16 * 16);  // [D]
+  short* ssrc = reinterpret_cast<short*>(sseg + (D + 3) / 4 * 4);                 // [R][9]
   const int m = (int)blockIdx.y + L.m_lo;
   const int r0 = L.seg[(m - L.m_lo) * D];
   const int r1 = (m + 1 <= L.lmax) ? L.seg[(m + 1 - L.m_lo) * D] : (int)L.nrows;
   const int R = r1 - r0;
   const long long w0 = (long long)blockIdx.x * W;
   const int tid = threadIdx.x, nth = blockDim.x;
-  // group rows staged with 8 loads in flight per thread
+  // group rows staged with 8 loads in flight per thread (asynchronous copies
+  // into the tile measured no faster here)
   for (int e0 = tid; e0 < R * W; e0 += 8 * nth) {
     C v[8];
 #pragma unroll
@@ -120,6 +122,17 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
   }
   for (int e = tid; e < R * 9; e += nth) sw[e] = tap_wr[(size_t)r0 * 9 + e];
   for (int e = tid; e < D; e += nth) sseg[e] = L.seg[(m - L.m_lo) * D + e] - r0;
+  // tap t = (l1 - l + 1) * 3 + (n2 + 1) of row r reads group row ssrc[r][t]
+  // (row 0 where the tap has no weight), so the tap loop below has no branches
+  const int am = abs(m), lmax = L.lmax;
+  for (int e = tid; e < R * 9; e += nth) {
+    const char4 q = L.rows[r0 + e / 9];
+    const int t = e % 9, l1 = q.x + t / 3 - 1, n1 = q.z - (t % 3 - 1), an1 = abs(n1);
+    int src = 0;
+    if (l1 >= 0 && l1 <= lmax && am <= l1 && an1 <= l1)
+      src = L.seg[(m - L.m_lo) * D + n1 + lmax] - r0 + l1 - (am > an1 ? am : an1);
+    ssrc[e] = (short)src;
+  }
   __syncthreads();
   const int w = tid % W, rl = tid / W, nrl = nth / W;
   const long long wg = w0 + w;
@@ -156,32 +169,26 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
     nu[q].x = my;
     nu[q].y = -mx;
   }
-  const int am = abs(m), lmax = L.lmax;
   for (int r = rl; r < R; r += nrl) {
-    const char4 q = L.rows[r0 + r];
-    const int l = q.x, n = q.z;
     const C f0 = tile[r * W + w];
     T ax = noise * f0.x, ay = noise * f0.y;
 #pragma unroll
     for (int n2o = 0; n2o < 3; ++n2o) {
-      const int n1 = n - (n2o - 1);
-      if (n1 < -lmax || n1 > lmax) continue;
-      const int an1 = abs(n1), lo = am > an1 ? am : an1;
-      const int base = sseg[n1 + lmax] - lo;
       T sx = 0, sy = 0;
 #pragma unroll
       for (int l1o = 0; l1o < 3; ++l1o) {
-        const T wt = sw[r * 9 + l1o * 3 + n2o];
-        if (wt != (T)0) {
-          const C fs = tile[(base + l + l1o - 1) * W + w];
-          sx += wt * fs.x;
-          sy += wt * fs.y;
-        }
+        const int t = r * 9 + l1o * 3 + n2o;
+        const T wt = sw[t];
+        const C fs = tile[ssrc[t] * W + w];
+        sx = fma(wt, fs.x, sx);
+        sy = fma(wt, fs.y, sy);
       }
       ax += nu[n2o].x * sx - nu[n2o].y * sy;
       ay += nu[n2o].x * sy + nu[n2o].y * sx;
     }
     if (sdk) {  // attitude diffusion: sum_o K^l[n][n+o-2] F^l_{m, n+o-2} (gyro-bias model)
+      const char4 q = L.rows[r0 + r];
+      const int l = q.x, n = q.z;
       const c2<T>* kw = sdk + (size_t)(r0 + r) * 5;
 #pragma unroll
       for (int o = 0; o < 5; ++o) {
@@ -208,7 +215,8 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
 
 template <typename T> static size_t local_smem(const hp_plan* p, int W) {
   const int rmax = (p->lmax + 1) * (p->lmax + 1);
-  return local_tile_bytes<T>(rmax, W) + ((size_t)rmax * 9 * sizeof(T) + 15) / 16 * 16 + sizeof(int) * p->D;
+  return local_tile_bytes<T>(rmax, W) + ((size_t)rmax * 9 * sizeof(T) + 15) / 16 * 16 +
+         sizeof(int) * ((p->D + 3) / 4 * 4) + sizeof(short) * (size_t)rmax * 9;
 }
 template <typename T> static const T* tap_table(const hp_plan* p);
 template <> const double* tap_table<double>(const hp_plan* p) { return p->tap_wr; }
@@ -265,10 +273,30 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
   const T inv_n2 = (T)1 / (T)(N * N);
 
   // ---- S1: load F rows n0-1 .. n0+cnt and P3 rows n0 .. n0+cnt-1 ----
-  // Loads are issued in fixed batches of 8 per thread before the shared-memory
-  // stores, so several requests are in flight per thread.
+  // Input already in the compute precision: asynchronous copies straight into
+  // the padded planes (every element's copy in flight at once, no register
+  // staging; rows outside -l..l are zero-filled).  FP64 input of an FP32 plan:
+  // loads in batches of 8 per thread, converted, then stored.
   const int nF = tl.cnt + 2;
-  {
+  if constexpr (sizeof(TIN) == sizeof(T)) {
+    const int tot = nF * N * N;
+    for (int e = tid; e < tot; e += nth) {
+      const int sl = e / (N * N), q = e % (N * N);
+      const int n = tl.n0 - 1 + sl;
+      const bool ok = n >= -tl.l && n <= tl.l;
+      const c2<TIN>* src = ok ? Fev + row_of(L, tl.l, tl.m, n) * L.nx + pbase + q : Fev;
+      cp_async<sizeof(C)>(sF + sl * PS + (q / N) * (N + 1) + q % N, src, ok);
+    }
+    if (HAS_P3) {
+      const int totp = tl.cnt * N * N;
+      for (int e = tid; e < totp; e += nth) {
+        const int sl = e / (N * N), q = e % (N * N);
+        cp_async<sizeof(C)>(sP + sl * PS + (q / N) * (N + 1) + q % N,
+                            P3 + row_of(L, tl.l, tl.m, tl.n0 + sl) * L.nx + pbase + q, true);
+      }
+    }
+    cp_async_wait_all();
+  } else {
     const int tot = nF * N * N;
     for (int e0 = tid; e0 < tot; e0 += 8 * nth) {
       C v[8];
@@ -291,7 +319,6 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
         }
       }
     }
-  }
   if (HAS_P3) {
     const int tot = tl.cnt * N * N;
     for (int e0 = tid; e0 < tot; e0 += 8 * nth) {
@@ -314,6 +341,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
         }
       }
     }
+  }
   }
   __syncthreads();
 
