@@ -44,7 +44,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_propagate_den', 'hp_state_hybrid_step', 'hp_pendulum_derivative_adjoint',
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
            'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info',
-           'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate']
+           'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate', 'hp_fftSO3_real_forward',
+           'hp_fftSO3_real_backward']
 
 
 class HPError(RuntimeError):
@@ -143,6 +144,8 @@ def _load():
         'hp_pendulum_adjoint': [vp, vp, vp, ip, dp, ip, ip, vp, ctypes.POINTER(hp_model_grad), ip],
         'hp_plan_set_gyro_bias_model': [vp, dp, vp, vp],
         'hp_gyrobias_propagate': [vp, vp, vp, dp, ip],
+        'hp_fftSO3_real_forward': [vp, vp, vp, ip, ip],
+        'hp_fftSO3_real_backward': [vp, vp, vp, ip, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -365,6 +368,48 @@ class Plan:
         pi, mi = _ptr(F, np.complex128)
         po, _ = _ptr(out, np.complex128)
         _check(_lib.hp_gyrobias_propagate(self._h, ctypes.c_void_p(pi), ctypes.c_void_p(po), float(dt), mi))
+        return out
+
+    def real_forward(self, f, out=None):
+        """Real-harmonic coefficients F(m, n, l[, b]) of fftSO3(f, B, true)
+        (fftSO3.m:61-119) for real SO(3) samples f(a, j, c[, b]) on this plan's
+        grid; a trailing axis batches independent functions."""
+        N, D = 2 * self.B, 2 * self.lmax + 1
+        f = _as_matlab(f, np.float64)
+        if isinstance(f, np.ndarray):
+            if tuple(f.shape[:3]) != (N, N, N) or f.ndim > 4:
+                raise HPError(HP_ERR_SHAPE, f'f must have shape ({N}, {N}, {N}[, nbatch])')
+            nb = f.shape[3] if f.ndim == 4 else 1
+        else:                                   # flat device tensor: nbatch from its size
+            nb = f.numel() // N ** 3
+            if nb * N ** 3 != f.numel() or nb < 1:
+                raise HPError(HP_ERR_SHAPE, f'f must hold nbatch * {N ** 3} values')
+        shape = (D, D, self.B) + ((nb,) if nb > 1 or getattr(f, 'ndim', 3) == 4 else ())
+        if out is None:
+            out = _empty_like_mem(f, shape, np.float64)
+        pf, mf = _ptr(f, np.float64)
+        po, _ = _ptr(out, np.float64)
+        _check(_lib.hp_fftSO3_real_forward(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(po), nb, mf))
+        return out
+
+    def real_backward(self, F, out=None):
+        """Real samples f(a, j, c[, b]) of ifftSO3(F, true) (ifftSO3.m:24-84)."""
+        N, D = 2 * self.B, 2 * self.lmax + 1
+        F = _as_matlab(F, np.float64)
+        if isinstance(F, np.ndarray):
+            if tuple(F.shape[:3]) != (D, D, self.B) or F.ndim > 4:
+                raise HPError(HP_ERR_SHAPE, f'F must have shape ({D}, {D}, {self.B}[, nbatch])')
+            nb = F.shape[3] if F.ndim == 4 else 1
+        else:
+            nb = F.numel() // (D * D * self.B)
+            if nb * D * D * self.B != F.numel() or nb < 1:
+                raise HPError(HP_ERR_SHAPE, f'F must hold nbatch * {D * D * self.B} values')
+        shape = (N, N, N) + ((nb,) if nb > 1 or getattr(F, 'ndim', 3) == 4 else ())
+        if out is None:
+            out = _empty_like_mem(F, shape, np.float64)
+        pF, mF = _ptr(F, np.float64)
+        po, _ = _ptr(out, np.float64)
+        _check(_lib.hp_fftSO3_real_backward(self._h, ctypes.c_void_p(pF), ctypes.c_void_p(po), nb, mF))
         return out
 
     def density_mf_gauss(self, U, s, V, mu, Sigma):
@@ -785,6 +830,18 @@ def ifftSO3R(F, isreal: bool = True, precision: int = HP_FP64):
     F = np.asarray(F)
     B, Bx, ndim = F.shape[2], F.shape[3] // 2, F.ndim - 3
     return get_plan(B, Bx, ndim, precision, HP_REAL if isreal else HP_COMPLEX).backward(F)
+
+
+def fftSO3_real(f):
+    """F = fftSO3(f, B, true): real-harmonic coefficients of real samples
+    f(a, j, c[, b]) (fftSO3.m:61-119), B = size(f, 1) / 2."""
+    B = np.asarray(f).shape[0] // 2
+    return get_plan(B, 2, 2).real_forward(f)
+
+
+def ifftSO3_real(F):
+    """f = ifftSO3(F, true) (ifftSO3.m:24-84), B = size(F, 3)."""
+    return get_plan(np.asarray(F).shape[2], 2, 2).real_backward(F)
 
 
 def fftSO3_prod(F, G):

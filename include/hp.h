@@ -208,6 +208,19 @@ int hp_pendulum_adjoint(hp_plan* plan, const double* F0, const double* lamT, int
 #define HP_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int hp_pendulum_derivative_noalloc(hp_plan* plan, const double* F, double* dF);
 
+/* Real-harmonic transforms of real functions on SO(3) alone (no omega axes),
+ * batched over nbatch independent functions on the plan's SO(3) grid (the
+ * plan's omega part is not used):
+ *   hp_fftSO3_real_forward  replaces  F = fftSO3(f, B, true)  (fftSO3.m:61-119)
+ *   hp_fftSO3_real_backward replaces  f = ifftSO3(F, true)    (ifftSO3.m:24-84)
+ * f: real (2B, 2B, 2B, nbatch), f(alpha, beta, gamma, b); F: real
+ * (2lmax+1, 2lmax+1, lmax+1, nbatch) in the real basis built from Wigner-d by
+ * the Psi table of fftSO3.m:62-88.  FP64 for every plan precision.  Callers:
+ * the SO(3)-only models (gyro_nobias.m) and fftSO3_deriv.m, whose derivative
+ * dF = sum_i eta_i F (u_i)^T uses getu(lmax, true) (getu.m:45-107). */
+int hp_fftSO3_real_forward(hp_plan* plan, const double* f, double* F, int nbatch, int mem);
+int hp_fftSO3_real_backward(hp_plan* plan, const double* F, double* f, int nbatch, int mem);
+
 /* Product rule of fftSO3_prod.m:209-265 (complex branch), batched over `batch`
  * independent pairs: FG^l = sum (2l1+1)(2l2+1)/(2l+1) [CG^T (F^l1 kron G^l2) CG]_l.
  * F, G, FG: (2lmax+1, 2lmax+1, lmax+1, batch) complex. */
