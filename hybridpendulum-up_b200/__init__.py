@@ -45,7 +45,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
            'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info',
            'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate', 'hp_fftSO3_real_forward',
-           'hp_fftSO3_real_backward']
+           'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod']
 
 
 class HPError(RuntimeError):
@@ -146,6 +146,7 @@ def _load():
         'hp_gyrobias_propagate': [vp, vp, vp, dp, ip],
         'hp_fftSO3_real_forward': [vp, vp, vp, ip, ip],
         'hp_fftSO3_real_backward': [vp, vp, vp, ip, ip],
+        'hp_fftSO3_real_prod': [vp, vp, vp, vp, ip, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -410,6 +411,19 @@ class Plan:
         pF, mF = _ptr(F, np.float64)
         po, _ = _ptr(out, np.float64)
         _check(_lib.hp_fftSO3_real_backward(self._h, ctypes.c_void_p(pF), ctypes.c_void_p(po), nb, mF))
+        return out
+
+    def real_prod(self, F, G, out=None):
+        """Real-harmonic coefficients of the product f g (fftSO3_prod.m:97-205,
+        isreal) from real coefficients F, G of shape (D, D, B[, batch])."""
+        D = 2 * self.lmax + 1
+        F = np.asfortranarray(np.asarray(F, dtype=np.float64))
+        G = np.asfortranarray(np.asarray(G, dtype=np.float64))
+        if F.shape != G.shape or tuple(F.shape[:3]) != (D, D, self.B) or F.ndim > 4:
+            raise HPError(HP_ERR_SHAPE, f'F and G must have shape ({D}, {D}, {self.B}[, batch])')
+        nb = F.shape[3] if F.ndim == 4 else 1
+        out = np.zeros(F.shape, order='F') if out is None else out
+        _check(_lib.hp_fftSO3_real_prod(self._h, F.ctypes.data, G.ctypes.data, out.ctypes.data, nb, HP_HOST))
         return out
 
     def density_mf_gauss(self, U, s, V, mu, Sigma):
@@ -842,6 +856,12 @@ def fftSO3_real(f):
 def ifftSO3_real(F):
     """f = ifftSO3(F, true) (ifftSO3.m:24-84), B = size(F, 3)."""
     return get_plan(np.asarray(F).shape[2], 2, 2).real_backward(F)
+
+
+def fftSO3_prod_real(F, G):
+    """FG of fftSO3_prod(func1, func2, B, true) (fftSO3_prod.m:97-205) from the
+    real-harmonic coefficients F, G of the two functions."""
+    return get_plan(np.asarray(F).shape[2], 2, 2).real_prod(F, G)
 
 
 def fftSO3_prod(F, G):

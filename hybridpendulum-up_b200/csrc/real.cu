@@ -280,3 +280,117 @@ extern "C" int hp_fftSO3_real_backward(hp_plan* p, const double* F, double* f, i
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HP_OK;
 }
+
+// ------------------------------------------------------- real product ----
+// fftSO3_prod.m:97-205 (isreal) builds real Clebsch-Gordan matrices from the
+// unitary T^l of lines 103-120; equivalently, with F_c^l = (T^l)^H F_r^l T^l the
+// complex coefficients of the same function, FG_r^l = Re T^l FG_c^l (T^l)^H for
+// the complex product FG_c (hp_fftSO3_prod).  T^l has two entries per row:
+//   r < 0 : T[r][r] = i/sqrt2,       T[r][-r] = -i (-1)^r / sqrt2
+//   r = 0 : T[0][0] = 1
+//   r > 0 : T[r][r] = (-1)^r/sqrt2,  T[r][-r] = 1/sqrt2
+__device__ __forceinline__ double2 t_entry(int r, int c) {
+  const double h = M_SQRT1_2, sr = (r & 1) ? -1.0 : 1.0;
+  if (r == 0) return make_double2(c == 0 ? 1.0 : 0.0, 0.0);
+  if (c == r) return r < 0 ? make_double2(0.0, h) : make_double2(sr * h, 0.0);
+  if (c == -r) return r < 0 ? make_double2(0.0, -sr * h) : make_double2(h, 0.0);
+  return make_double2(0.0, 0.0);
+}
+
+// Fc[m][n] = sum_{p in {m,-m}, q in {n,-n}} conj(T[p][m]) Fr[p][q] T[q][n]
+__global__ void k_real_to_cplx(int B, int nb, const double* __restrict__ Fr, double2* __restrict__ Fc) {
+  const int lmax = B - 1, D = 2 * lmax + 1;
+  const long long per = (long long)D * D * (lmax + 1);
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= per * nb) return;
+  const int m = (int)(t % D) - lmax, n = (int)((t / D) % D) - lmax;
+  const int l = (int)((t / ((long long)D * D)) % (lmax + 1));
+  const long long base = t - ((long long)(m + lmax) + (long long)D * (n + lmax));
+  double2 acc = make_double2(0.0, 0.0);
+  if (abs(m) <= l && abs(n) <= l) {
+    for (int ip = 0; ip < (m == 0 ? 1 : 2); ++ip) {
+      const int p = ip ? -m : m;
+      const double2 a = t_entry(p, m);              // T[p][m], conjugated below
+      for (int iq = 0; iq < (n == 0 ? 1 : 2); ++iq) {
+        const int q = iq ? -n : n;
+        const double2 b = t_entry(q, n);
+        const double v = Fr[base + (p + lmax) + (long long)D * (q + lmax)];
+        // conj(a) * v * b
+        const double2 ab = make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+        acc.x += v * ab.x;
+        acc.y += v * ab.y;
+      }
+    }
+  }
+  Fc[t] = acc;
+}
+
+// Xr[m][n] = Re sum_{p in {m,-m}, q in {n,-n}} T[m][p] Xc[p][q] conj(T[n][q])
+__global__ void k_cplx_to_real(int B, int nb, const double2* __restrict__ Xc, double* __restrict__ Xr) {
+  const int lmax = B - 1, D = 2 * lmax + 1;
+  const long long per = (long long)D * D * (lmax + 1);
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= per * nb) return;
+  const int m = (int)(t % D) - lmax, n = (int)((t / D) % D) - lmax;
+  const int l = (int)((t / ((long long)D * D)) % (lmax + 1));
+  const long long base = t - ((long long)(m + lmax) + (long long)D * (n + lmax));
+  double acc = 0.0;
+  if (abs(m) <= l && abs(n) <= l) {
+    for (int ip = 0; ip < (m == 0 ? 1 : 2); ++ip) {
+      const int p = ip ? -m : m;
+      const double2 a = t_entry(m, p);
+      for (int iq = 0; iq < (n == 0 ? 1 : 2); ++iq) {
+        const int q = iq ? -n : n;
+        const double2 b = t_entry(n, q);                 // conjugated below
+        const double2 x = Xc[base + (p + lmax) + (long long)D * (q + lmax)];
+        const double2 ax = make_double2(a.x * x.x - a.y * x.y, a.x * x.y + a.y * x.x);
+        acc += ax.x * b.x + ax.y * b.y;                  // Re(ax * conj(b))
+      }
+    }
+  }
+  Xr[t] = acc;
+}
+
+extern "C" int hp_fftSO3_real_prod(hp_plan* p, const double* F, const double* G, double* FG, int batch, int mem) {
+  HP_CHECK(real_args(p, F, G, batch, mem));
+  if (!FG) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  const int B = p->B, D = p->D;
+  const size_t n = (size_t)D * D * B * batch;
+  int st = HP_OK;
+  double2* Fc = (double2*)p->ws_get("realprod.Fc", sizeof(double2) * n, &st);
+  if (st) return st;
+  double2* Gc = (double2*)p->ws_get("realprod.Gc", sizeof(double2) * n, &st);
+  if (st) return st;
+  double2* FGc = (double2*)p->ws_get("realprod.FGc", sizeof(double2) * n, &st);
+  if (st) return st;
+  const double *Fd = F, *Gd = G;
+  double* FGd = FG;
+  if (mem == HP_HOST) {
+    double* a = (double*)p->ws_get("realprod.F", sizeof(double) * n, &st);
+    if (st) return st;
+    double* b = (double*)p->ws_get("realprod.G", sizeof(double) * n, &st);
+    if (st) return st;
+    FGd = (double*)p->ws_get("realprod.FG", sizeof(double) * n, &st);
+    if (st) return st;
+    HP_CUDA_TRY(cudaMemcpyAsync(a, F, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
+    HP_CUDA_TRY(cudaMemcpyAsync(b, G, sizeof(double) * n, cudaMemcpyHostToDevice, p->stream));
+    Fd = a;
+    Gd = b;
+  }
+  const unsigned g = (unsigned)((n + 127) / 128);
+  {
+    ProfScope _ps(p, "real.prod", p->stream);
+    k_real_to_cplx<<<g, 128, 0, p->stream>>>(B, batch, Fd, Fc);
+    k_real_to_cplx<<<g, 128, 0, p->stream>>>(B, batch, Gd, Gc);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  HP_CHECK(hp_prod_launch(p, Fc, Gc, FGc, batch, p->stream));
+  {
+    ProfScope _ps(p, "real.prod", p->stream);
+    k_cplx_to_real<<<g, 128, 0, p->stream>>>(B, batch, FGc, FGd);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  if (mem == HP_HOST) HP_CUDA_TRY(cudaMemcpyAsync(FG, FGd, sizeof(double) * n, cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return HP_OK;
+}

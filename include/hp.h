@@ -220,6 +220,11 @@ int hp_pendulum_derivative_noalloc(hp_plan* plan, const double* F, double* dF);
  * dF = sum_i eta_i F (u_i)^T uses getu(lmax, true) (getu.m:45-107). */
 int hp_fftSO3_real_forward(hp_plan* plan, const double* f, double* F, int nbatch, int mem);
 int hp_fftSO3_real_backward(hp_plan* plan, const double* F, double* f, int nbatch, int mem);
+/* Product rule in the real basis, fftSO3_prod(func1, func2, B, true)
+ * (fftSO3_prod.m:97-205): FG from real F, G (2lmax+1, 2lmax+1, lmax+1, batch).
+ * Computed as Re T FG_c T^H with FG_c the complex product (hp_fftSO3_prod) of
+ * F_c = T^H F T, G_c = T^H G T, T^l the unitary of fftSO3_prod.m:103-120. */
+int hp_fftSO3_real_prod(hp_plan* plan, const double* F, const double* G, double* FG, int batch, int mem);
 
 /* Product rule of fftSO3_prod.m:209-265 (complex branch), batched over `batch`
  * independent pairs: FG^l = sum (2l1+1)(2l2+1)/(2l+1) [CG^T (F^l1 kron G^l2) CG]_l.

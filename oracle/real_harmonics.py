@@ -147,3 +147,45 @@ def deriv(F: np.ndarray, eta) -> np.ndarray:
         for i in range(3):
             dF[s, s, l] += eta[i] * F[s, s, l] @ u[s, s, l, i].T
     return dF
+
+
+def t_matrix(l: int) -> np.ndarray:
+    """Real-to-complex basis matrix T^l of fftSO3_prod.m:103-120 (unitary):
+    the complex coefficients are F_c^l = (T^l)^H F_r^l T^l."""
+    T = np.zeros((2 * l + 1, 2 * l + 1), complex)
+    for m in range(-l, l + 1):
+        if m < 0:
+            T[m + l, m + l] = 1j
+            T[m + l, -m + l] = -1j * (-1.0) ** (-m)
+        elif m == 0:
+            T[l, l] = math.sqrt(2.0)
+        else:
+            T[m + l, m + l] = (-1.0) ** m
+            T[m + l, -m + l] = 1.0
+    return T / math.sqrt(2.0)
+
+
+def prod_literal(F: np.ndarray, G: np.ndarray) -> np.ndarray:
+    """FG of fftSO3_prod.m:97-205 (isreal) from real coefficients F, G: the
+    real Clebsch-Gordan matrices cg = kron(conj T1, conj T2) CG blkdiag(T)^T and
+    A = (2l1+1)(2l2+1) cg^T kron(F^l1, G^l2) conj(cg), l-blocks / (2l+1), real part."""
+    lmax = F.shape[2] - 1
+    FG = np.zeros(F.shape, complex)
+    for l1 in range(lmax + 1):
+        for l2 in range(lmax + 1):
+            CG = so3.clebsch_gordan(l1, l2)
+            Tb = np.zeros((CG.shape[1], CG.shape[1]), complex)
+            o = 0
+            for l in range(abs(l1 - l2), l1 + l2 + 1):
+                Tb[o:o + 2 * l + 1, o:o + 2 * l + 1] = t_matrix(l)
+                o += 2 * l + 1
+            cg = np.kron(np.conj(t_matrix(l1)), np.conj(t_matrix(l2))) @ CG @ Tb.T
+            i1 = slice(lmax - l1, lmax + l1 + 1)
+            i2 = slice(lmax - l2, lmax + l2 + 1)
+            A = cg.T @ np.kron(F[i1, i1, l1], G[i2, i2, l2]) @ np.conj(cg)
+            A = A * (2 * l1 + 1) * (2 * l2 + 1)
+            for l in range(abs(l1 - l2), min(l1 + l2, lmax) + 1):
+                s = l * l - (l1 - l2) ** 2
+                iF = slice(lmax - l, lmax + l + 1)
+                FG[iF, iF, l] += A[s:s + 2 * l + 1, s:s + 2 * l + 1] / (2 * l + 1)
+    return FG.real

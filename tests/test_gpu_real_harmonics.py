@@ -71,3 +71,15 @@ def test_real_transform_errors(hp):
         plan.real_forward(np.zeros((5, 6, 6)))
     with pytest.raises(hp.HPError):
         plan.real_backward(np.zeros((5, 5, 2)))
+
+
+@pytest.mark.parametrize('B', [3, 5, 8])
+def test_real_product_vs_oracle(hp, B):
+    f, g = band_limited(B, 7), band_limited(B, 8)
+    F, G = rh.forward(f), rh.forward(g)
+    ref = rh.prod_literal(F, G)
+    out = hp.fftSO3_prod_real(F, G)
+    assert rmax(out, ref) < 1e-11
+    # batched
+    FG2 = hp.get_plan(B, 2, 2).real_prod(np.stack([F, G], -1), np.stack([G, F], -1))
+    assert rmax(FG2[..., 0], ref) < 1e-11 and rmax(FG2[..., 1], ref) < 1e-11

@@ -53,3 +53,18 @@ def test_real_lie_derivative_matches_complex(eta):
     df_c = so3.ifftSO3R_backward(dFc, real=True)
     df_r = rh.backward(rh.deriv(rh.forward(f), eta))
     assert np.abs(df_r - df_c).max() <= 1e-12 * np.abs(df_c).max()
+
+
+def test_real_product_literal_equals_basis_change():
+    """fftSO3_prod.m's real Clebsch-Gordan route = Re T (complex product) T^H."""
+    B = 4
+    lmax = B - 1
+    f, g = band_limited(B, 1), band_limited(B, 2)
+    FGr = rh.prod_literal(rh.forward(f), rh.forward(g))
+    FGc = so3.fftSO3_prod(so3.fftSO3R_forward(f), so3.fftSO3R_forward(g))
+    ref = np.zeros_like(FGr)
+    for l in range(lmax + 1):
+        s = slice(lmax - l, lmax + l + 1)
+        T = rh.t_matrix(l)
+        ref[s, s, l] = (T @ FGc[s, s, l] @ T.conj().T).real
+    assert np.abs(FGr - ref).max() <= 1e-13 * np.abs(FGr).max()
