@@ -27,6 +27,10 @@
 #include "mex.h"
 #include "hp.h"
 
+#ifndef M_PI   /* not in strict ISO C */
+#define M_PI 3.14159265358979323846
+#endif
+
 #ifdef HP_MEX_MIXED
 #define HP_MEX_PRECISION HP_MIXED
 #else

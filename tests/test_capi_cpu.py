@@ -66,3 +66,23 @@ def test_mex_argument_checks(hp):
     x = pd.omega_grid(3, P.L, 3)
     with pytest.raises(hp.HPError):
         hp._fit_gyro(pd.make_OJO(x, Jfull), 3, P.L)
+
+
+@pytest.mark.parametrize('gateway', ['HP_MEX_PROPAGATE3', 'HP_MEX_PROPAGATE2', 'HP_MEX_FFTSO3R',
+                                     'HP_MEX_GYROBIAS'])
+def test_mex_gateway_compiles(gateway):
+    """The MATLAB gateways (one source, one define each) compile against
+    include/hp.h and the MEX API declarations (MATLAB itself is not installed)."""
+    import shutil
+    import subprocess
+    cc = shutil.which('gcc')
+    if cc is None:
+        pytest.skip('no C compiler')
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    src = os.path.join(root, 'hybridpendulum-up_b200', 'mex', 'hp_mex.c')
+    for extra in ([], ['-DHP_MEX_MIXED']):
+        r = subprocess.run([cc, '-std=c99', '-Wall', '-Werror', '-fsyntax-only', f'-D{gateway}', *extra,
+                            '-I', os.path.join(here, 'mex_stub'), '-I', os.path.join(root, 'include'), src],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
