@@ -32,6 +32,7 @@ struct hp_batch {
   double dt = 0.0;
   int method = -1;
   std::vector<double2*> capF;               // each member's F at capture
+  std::vector<int> capF32;                  // and its FP32-copy state: valid * 2 + current slot
   long long graph_launches = 0;
 };
 
@@ -73,15 +74,23 @@ int batch_step(hp_batch* b, double dt, int method) {
   return HP_OK;
 }
 
+// The replayed graph reads the FP32 copy the capture saw as valid: a member
+// whose copy was invalidated (or whose slot moved) since must step eagerly.
+int f32_tag(const hp_state* s) { return (s->f32_valid ? 2 : 0) + s->f32_cur; }
+
 bool at_capture_buffers(const hp_batch* b) {
   for (size_t i = 0; i < b->st.size(); ++i)
-    if (b->st[i]->F != b->capF[i]) return false;
+    if (b->st[i]->F != b->capF[i] || f32_tag(b->st[i]) != b->capF32[i]) return false;
   return true;
 }
 
 int capture(hp_batch* b, double dt, int method) {
   b->capF.clear();
-  for (auto s : b->st) b->capF.push_back(s->F);
+  b->capF32.clear();
+  for (auto s : b->st) {
+    b->capF.push_back(s->F);
+    b->capF32.push_back(f32_tag(s));
+  }
   std::vector<bool> fg(b->st.size());
   for (size_t i = 0; i < b->st.size(); ++i) fg[i] = b->st[i]->fg_valid;
   HP_CUDA_TRY(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeRelaxed));
@@ -95,7 +104,10 @@ int capture(hp_batch* b, double dt, int method) {
   HP_CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
   // capturing enqueued nothing: the buffers are back where they started
   for (size_t i = 0; i < b->st.size(); ++i) {
-    if (b->st[i]->F != b->capF[i]) { hp_set_error("state buffers do not cycle with period two"); return HP_ERR_UNSUPPORTED; }
+    if (b->st[i]->F != b->capF[i] || f32_tag(b->st[i]) != b->capF32[i]) {
+      hp_set_error("state buffers do not cycle with period two");
+      return HP_ERR_UNSUPPORTED;
+    }
     b->st[i]->fg_valid = fg[i];
   }
   b->dt = dt;

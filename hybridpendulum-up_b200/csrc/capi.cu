@@ -449,32 +449,35 @@ extern "C" int hp_fftSO3R_backward(hp_plan* p, const double* F, double* f, int m
 // fgrid: grid density of *F for the first stage of a density-gravity model
 // (null: recomputed from *F), as pendulum_reduced_den.m:359-399 passes f to the
 // first derivative only.
+// fin32 (may be null): *F already in FP32, read by the first derivative
+// evaluation; fout32 (may be null): receives the new F in FP32 from the last one.
 static int integrate_internal(hp_plan* p, double2** F, double2** F2, double2** F3, double2* acc, double dt,
-                              int method, const void* fgrid = nullptr) {
+                              int method, const void* fgrid = nullptr, const void* fin32 = nullptr,
+                              void* fout32 = nullptr) {
   cudaStream_t s = p->stream;
   const size_t bytes = 16 * (size_t)p->nrows * p->nx;
   switch (method) {
     case HP_EULER:
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, nullptr, 0.0, s, fgrid));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, nullptr, 0.0, s, fgrid, fin32, fout32));
       std::swap(*F, *F2);
       return HP_OK;
     case HP_MIDPOINT:
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, nullptr, 0.0, s, fgrid));
-      HP_CHECK(hp_derivative_eval(p, *F2, *F, dt, *F3, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, nullptr, 0.0, s, fgrid, fin32));
+      HP_CHECK(hp_derivative_eval(p, *F2, *F, dt, *F3, nullptr, 0.0, s, nullptr, nullptr, fout32));
       std::swap(*F, *F3);
       return HP_OK;
     case HP_RK2:
       HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, acc, dt / 2, s, fgrid));
-      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 2, *F3, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt, *F2, acc, dt / 2, s, fgrid, fin32));
+      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 2, *F3, nullptr, 0.0, s, nullptr, nullptr, fout32));
       std::swap(*F, *F3);
       return HP_OK;
     case HP_RK4:
       HP_CUDA_TRY(cudaMemcpyAsync(acc, *F, bytes, cudaMemcpyDeviceToDevice, s));
-      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, acc, dt / 6, s, fgrid));
+      HP_CHECK(hp_derivative_eval(p, *F, *F, dt / 2, *F2, acc, dt / 6, s, fgrid, fin32));
       HP_CHECK(hp_derivative_eval(p, *F2, *F, dt / 2, *F3, acc, dt / 3, s));
       HP_CHECK(hp_derivative_eval(p, *F3, *F, dt, *F2, acc, dt / 3, s));
-      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 6, *F3, nullptr, 0.0, s));
+      HP_CHECK(hp_derivative_eval(p, *F2, acc, dt / 6, *F3, nullptr, 0.0, s, nullptr, nullptr, fout32));
       std::swap(*F, *F3);
       return HP_OK;
     default:
@@ -617,6 +620,7 @@ extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
 extern "C" int hp_state_destroy(hp_state* s) {
   if (!s) return HP_OK;
   cudaFree(s->F); cudaFree(s->F2); cudaFree(s->F3); cudaFree(s->acc); cudaFree(s->fg);
+  cudaFree(s->F32[0]); cudaFree(s->F32[1]);
   delete s;
   return HP_OK;
 }
@@ -631,6 +635,7 @@ extern "C" int hp_state_load(hp_state* s, const double* F, int mem) {
   HP_CHECK(hp_full_to_internal(p, d, s->F, p->stream));
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   s->fg_valid = false;
+  s->f32_valid = false;
   return HP_OK;
 }
 
@@ -667,7 +672,32 @@ extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
   if (method < HP_EULER || method > HP_RK4) { hp_set_error("bad method"); return HP_ERR_INVALID; }
   HP_CHECK(state_bufs(s, method));
   if (nsteps > 0) s->fg_valid = false;
-  for (int k = 0; k < nsteps; ++k) HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
+  // Mixed 3-D plans carry F in FP32 from step to step: the last plane pass of
+  // a step writes it, the next step's first evaluation and the density read it.
+  const bool carry = p->ndim == 3 && p->precision == HP_MIXED;
+  if (carry && !s->F32[0]) {
+    const size_t b32 = 8 * (size_t)p->nrows * p->nx;
+    if (cudaMalloc(&s->F32[0], b32) != cudaSuccess || cudaMalloc(&s->F32[1], b32) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(s->F32[0]); cudaFree(s->F32[1]);
+      s->F32[0] = s->F32[1] = nullptr;
+      hp_set_error("device allocation failed");
+      return HP_ERR_ALLOC;
+    }
+    s->f32_valid = false;
+  }
+  for (int k = 0; k < nsteps; ++k) {
+    if (carry) {
+      const float2* in = s->f32_valid ? s->F32[s->f32_cur] : nullptr;
+      s->f32_valid = false;
+      HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method, nullptr, in,
+                                  s->F32[1 - s->f32_cur]));
+      s->f32_cur = 1 - s->f32_cur;
+      s->f32_valid = true;
+    } else {
+      HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
+    }
+  }
   return HP_OK;
 }
 
@@ -679,6 +709,7 @@ extern "C" int hp_state_load_density(hp_state* s, const void* f) {
   hp_plan* p = s->plan;
   HP_CHECK(hp_forward_internal(p, f, p->symmetry == HP_COMPLEX, s->F, p->stream));
   s->fg_valid = false;
+  s->f32_valid = false;
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HP_OK;
 }
@@ -703,6 +734,7 @@ extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int
       return HP_ERR_ALLOC;
     }
   }
+  if (nsteps > 0) s->f32_valid = false;   // the forward transform below rewrites F
   if (!s->fg_valid && nsteps > 0) HP_CHECK(hp_backward_internal(p, s->F, s->fg, 0, st));
   for (int k = 0; k < nsteps; ++k) {
     s->fg_valid = false;
@@ -725,6 +757,8 @@ extern "C" int hp_state_density(hp_state* s, void* f) {
     HP_CUDA_TRY(cudaMemcpyAsync(f, s->fg, eb * (size_t)p->n_grid(), cudaMemcpyDeviceToDevice, p->stream));
     return HP_OK;
   }
+  if (s->f32_valid)   // the FP32 copy the last step left: the values the FP32 transform converts to
+    return hp_backward_internal32(p, s->F32[s->f32_cur], f, p->symmetry == HP_COMPLEX, p->stream);
   return hp_backward_internal(p, s->F, f, p->symmetry == HP_COMPLEX, p->stream);
 }
 
@@ -742,6 +776,7 @@ extern "C" int hp_state_normalize(hp_state* s, double mass, double* scale) {
   const double f = mass / m0;
   const long long n = p->nrows * p->nx;
   s->fg_valid = false;
+  s->f32_valid = false;
   {
     ProfScope _ps(p, "normalize", p->stream);
     k_scale_c64<<<(unsigned)((n + 255) / 256), 256, 0, p->stream>>>(s->F, n, f);

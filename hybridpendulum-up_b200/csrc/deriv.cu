@@ -42,19 +42,21 @@ using namespace hp;
 
 // -------------------------------------------------------- pass A: axis 3 ----
 // Fc (may be null): the coefficients themselves in the compute precision, the
-// input the local and plane passes then read instead of the FP64 state.
-template <int N, typename T>
-__global__ void __launch_bounds__(128) k_axis3(RowLayout L, const double2* __restrict__ F,
+// input the local and plane passes then read instead of the FP64 state.  With
+// TIN = T the input already is that copy (written by the previous step's plane
+// pass) and Fc is null.
+template <int N, typename T, typename TIN = double>
+__global__ void __launch_bounds__(128) k_axis3(RowLayout L, const c2<TIN>* __restrict__ F,
                                                c2<T>* __restrict__ P3, T Llen, c2<T>* __restrict__ Fc) {
   using C = c2<T>;
   constexpr long long plane = (long long)N * N;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= L.nrows * plane) return;
   const long long row = t / plane, p = t % plane;
-  const double2* src = F + row * L.nx + p;
+  const c2<TIN>* src = F + row * L.nx + p;
   C x[N];
 #pragma unroll
-  for (int j = 0; j < N; ++j) x[j] = cvt<C, double2>(__ldg(src + j * plane));
+  for (int j = 0; j < N; ++j) x[j] = cvt<C, c2<TIN>>(__ldg(src + j * plane));
   if (Fc) {
     C* fc = Fc + row * L.nx + p;
 #pragma unroll
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
                                                   const double2* __restrict__ F0, double a,
                                                   double2* __restrict__ out,
                                                   double2* __restrict__ acc, double bacc,
-                                                  DerivParams prm) {
+                                                  DerivParams prm, c2<T>* __restrict__ out32 = nullptr) {
   using C = c2<T>;
   constexpr int CT = PlaneCfg<T>::C;
   constexpr int PS = N * (N + 1);
@@ -509,6 +511,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
         o.x += a * dx;
         o.y += a * dy;
         out[gi[u]] = o;
+        if (out32) out32[gi[u]] = cvt<C, double2>(o);   // the next step's compute-precision input
         if (acc) {
           double2 v = ac[u];
           v.x += bacc * dx;
@@ -561,7 +564,8 @@ static int launch_local(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* Gx,
 
 template <int N, typename T>
 static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                       double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
+                       double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx,
+                       const void* fev32, void* out32) {
   using C = c2<T>;
   int st = HP_OK;
   const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
@@ -575,8 +579,13 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   // mixed 3-D plans: the axis-3 pass also leaves F in FP32 (Fc), which the
   // local and plane passes read in place of the FP64 state (the values they
   // convert to anyway), halving their coefficient traffic
+  // When the caller already holds Fev in FP32 (fev32, from the previous step's
+  // plane pass), the axis-3 pass reads that copy and writes none.
+  const bool mixed3 = p->ndim == 3 && sizeof(T) == 4;
   C* Fc = nullptr;
-  if (p->ndim == 3 && sizeof(T) == 4) {
+  if (mixed3 && fev32) {
+    Fc = (C*)const_cast<void*>(fev32);
+  } else if (mixed3) {
     Fc = (C*)p->ws_get("deriv.F32", fb, &st);
     if (st) return st;
   }
@@ -584,7 +593,10 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   if (p->ndim == 3) {
     const long long nt = p->nrows * (long long)N * N;
     ProfScope _ps(p, "deriv.axis3", s);
-    k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L, Fc);
+    if (mixed3 && fev32)
+      k_axis3<N, T, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fc, P3, (T)prm.L, (C*)nullptr);
+    else
+      k_axis3<N, T><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(L, Fev, P3, (T)prm.L, Fc);
     HP_CUDA_TRY(cudaGetLastError());
   }
   if (Fc) {
@@ -613,7 +625,8 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
   ProfScope _ps(p, "deriv.plane", s);
   if (p3 && Fc) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_plane<N, T, true, T><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fc, P3, G, F0, a, out, acc, bacc, prm);
+    k_plane<N, T, true, T><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fc, P3, G, F0, a, out, acc, bacc, prm,
+                                                                (C*)(mixed3 ? out32 : nullptr));
   } else if (p3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_plane<N, T, true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_plane<N, T, true, double><<<grid, PlaneCfg<T>::NT, smem, s>>>(L, dt, Fev, P3, G, F0, a, out, acc, bacc, prm);
@@ -723,17 +736,18 @@ static int run_deriv_lines(hp_plan* p, const double2* Fev, const double2* F0, do
 
 template <typename T>
 static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                     double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx) {
+                     double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx,
+                     const void* fev32 = nullptr, void* out32 = nullptr) {
   switch (p->N) {
-    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 30: return run_deriv_N<30, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
-    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 30: return run_deriv_N<30, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
     case 40: case 48: case 60: return run_deriv_lines<T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     default:
       hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24, 30 or 32)");
@@ -807,7 +821,8 @@ DerivParams hp_model_params(const hp_plan* p) {
 }
 
 int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Fev, const double2* F0, double a,
-                           double2* out, double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
+                           double2* out, double2* acc, double bacc, cudaStream_t s, const void* fgrid,
+                           const void* fev32, void* out32) {
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   const bool den = p->den_mR != nullptr && (prm.gs[0] != 0 || prm.gs[1] != 0);
@@ -818,15 +833,16 @@ int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Fe
   }
   float2* Gx = nullptr;
   if (den) HP_CHECK_RET(den_gravity<float>(p, Fev, fgrid, s, &Gx));
-  return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+  return run_deriv<float>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
 }
 
 // out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
 // With a density-gravity model (hp_pendulum_propagate_den), fgrid is the grid
 // density of Feval when the caller has it (else it is recomputed from Feval).
 int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
-                       double2* acc, double bacc, cudaStream_t s, const void* fgrid) {
-  return hp_derivative_eval_prm(p, hp_model_params(p), Fev, F0, a, out, acc, bacc, s, fgrid);
+                       double2* acc, double bacc, cudaStream_t s, const void* fgrid, const void* fev32,
+                       void* out32) {
+  return hp_derivative_eval_prm(p, hp_model_params(p), Fev, F0, a, out, acc, bacc, s, fgrid, fev32, out32);
 }
 
 // ------------------------------------------ derivative without allocation ----

@@ -179,6 +179,7 @@ extern "C" int hp_state_init_mf_gauss(hp_state* sta, const double* U, const doub
   st = hp_forward_internal64(p, f, sta->F, p->stream);
   if (st) return st;
   sta->fg_valid = false;
+  sta->f32_valid = false;
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   // the FP64 grid density and transform buffers are only needed here
   for (const char* k : {"init.f", "tf.t1", "tf.t2"}) p->ws_release(k);

@@ -94,6 +94,11 @@ struct hp_state {
   double2* acc = nullptr;
   void* fg = nullptr;       // grid density of the hybrid step (compute precision)
   bool fg_valid = false;    // fg holds the post-collision density of F
+  // mixed 3-D plans: F converted to FP32 by the last plane pass of a step,
+  // ping-pong pair; F32[f32_cur] is valid for the current F when f32_valid
+  float2* F32[2] = {nullptr, nullptr};
+  int f32_cur = 0;
+  bool f32_valid = false;
 };
 
 struct hp_collision;
@@ -137,12 +142,16 @@ struct DerivParams {
   double mr[3][3][2];  // MR_i^1_{0 n2}: [n2+1][i][re, im]
 };
 DerivParams hp_model_params(const hp_plan* p);
+// fev32 (mixed 3-D plans, may be null): Feval already converted to FP32 in the
+// [row][omega] layout; out32 (may be null): receives out converted to FP32.
 int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Feval, const double2* F0,
                            double a, double2* out, double2* acc, double bacc, cudaStream_t s,
-                           const void* fgrid = nullptr);
+                           const void* fgrid = nullptr, const void* fev32 = nullptr, void* out32 = nullptr);
 int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, double a,
                        double2* out, double2* acc, double bacc, cudaStream_t s,
-                       const void* fgrid = nullptr);
+                       const void* fgrid = nullptr, const void* fev32 = nullptr, void* out32 = nullptr);
+// backward transform from FP32 coefficients in the [row][omega] layout (mixed plans)
+int hp_backward_internal32(hp_plan* p, const float2* Fint32, void* f, int complex_out, cudaStream_t s);
 // Forward transform of mult . f (mult: (2B)^3 grid samples, may be null) into
 // [row][omega] coefficients in the plan's compute precision (c2<T>).
 int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* out, cudaStream_t s);

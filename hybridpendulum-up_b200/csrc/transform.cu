@@ -864,6 +864,18 @@ int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_o
   return backward_T<float>(p, Fint, f, complex_out, s);
 }
 
+int hp_backward_internal32(hp_plan* p, const float2* Fint32, void* f, int complex_out, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  if (p->precision != HP_MIXED) { hp_set_error("FP32 coefficients need a mixed-precision plan"); return HP_ERR_INVALID; }
+  int st = HP_OK;
+  float2* t1 = (float2*)p->ws_get("tf.t1", sizeof(float2) * (size_t)p->nrows * p->nx, &st);
+  if (st) return st;
+  st = omega_fft_any<float, float>(p, Fint32, t1, true, s);
+  if (st) return st;
+  if (complex_out) return synth_any<float, true>(p, t1, f, s);
+  return synth_any<float, false>(p, t1, f, s);
+}
+
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   if (p->precision == HP_FP64) return forward_T<double>(p, f, complex_in, Fint, s);
