@@ -198,57 +198,71 @@ __device__ __forceinline__ void fft_stages(C (&x)[N]) {
   }
 }
 
-// 30 = 2 * 3 * 5 by the prime-factor (Good-Thomas) algorithm, no twiddles:
-// with n = (15 n1 + 10 n2 + 6 n3) mod 30 and k = (15 k1 + 10 k2 + 6 k3) mod 30,
-// nk = 15 n1k1 + 10 n2k2 + 6 n3k3 (mod 30), so the 30-point DFT is a 2 x 3 x 5
-// DFT over (n1, n2, n3) with both index maps applied as register permutations.
-template <bool INV, typename C>
-__device__ __forceinline__ void fft30_pfa(C (&x)[30]) {
-  C y[30];   // y[(n1 * 3 + n2) * 5 + n3] = x[(15 n1 + 10 n2 + 6 n3) % 30]
+// Prime-factor (Good-Thomas) FFT for N = N1 N2 N3 with pairwise coprime
+// factors, no twiddle multiplies.  Input map n = (N/N1 n1 + N/N2 n2 + N/N3 n3)
+// mod N; output map k = (M1 k1 + M2 k2 + M3 k3) mod N with Mi = N/Ni times the
+// inverse of N/Ni modulo Ni (Chinese remainder), so that
+// nk = (N/N1)M1 n1k1 + ... = N/N1 n1k1 + ... (mod N) and the N-point DFT is an
+// N1 x N2 x N3 DFT over (n1, n2, n3); both maps are register permutations.
+// Used for N = 30 (2*3*5, the 2B-point FFTs of B = 15) and N = 60 (4*3*5).
+template <int A, int M> constexpr int inv_mod() {
+  int r = 1;
+  while ((A % M) * r % M != 1) ++r;
+  return r;
+}
+template <int N1, int N2, int N3, bool INV, typename C>
+__device__ __forceinline__ void fft_pfa3(C (&x)[N1 * N2 * N3]) {
+  constexpr int N = N1 * N2 * N3;
+  constexpr int Q1 = N / N1, Q2 = N / N2, Q3 = N / N3;
+  constexpr int M1 = Q1 * inv_mod<Q1, N1>(), M2 = Q2 * inv_mod<Q2, N2>(), M3 = Q3 * inv_mod<Q3, N3>();
 #pragma unroll
-  for (int n1 = 0; n1 < 2; ++n1)
+  for (int a = 0; a < N1 * N2; ++a) {   // length-N3 DFTs along n3
+    const int n1 = a / N2, n2 = a % N2;
+    C v[N3];
 #pragma unroll
-    for (int n2 = 0; n2 < 3; ++n2)
+    for (int r = 0; r < N3; ++r) v[r] = x[(Q1 * n1 + Q2 * n2 + Q3 * r) % N];
+    dft_small<N3, INV>(v);
 #pragma unroll
-      for (int n3 = 0; n3 < 5; ++n3) y[(n1 * 3 + n2) * 5 + n3] = x[(15 * n1 + 10 * n2 + 6 * n3) % 30];
+    for (int r = 0; r < N3; ++r) x[(Q1 * n1 + Q2 * n2 + Q3 * r) % N] = v[r];
+  }
+  // x now holds, at input position (n1, n2, k3), the partial result; continue in place
 #pragma unroll
-  for (int a = 0; a < 6; ++a) {   // length-5 DFTs along n3
-    C v[5];
+  for (int a = 0; a < N1 * N3; ++a) {   // length-N2 DFTs along n2
+    const int n1 = a / N3, k3 = a % N3;
+    C v[N2];
 #pragma unroll
-    for (int r = 0; r < 5; ++r) v[r] = y[a * 5 + r];
-    dft_small<5, INV>(v);
+    for (int r = 0; r < N2; ++r) v[r] = x[(Q1 * n1 + Q2 * r + Q3 * k3) % N];
+    dft_small<N2, INV>(v);
 #pragma unroll
-    for (int r = 0; r < 5; ++r) y[a * 5 + r] = v[r];
+    for (int r = 0; r < N2; ++r) x[(Q1 * n1 + Q2 * r + Q3 * k3) % N] = v[r];
   }
 #pragma unroll
-  for (int n1 = 0; n1 < 2; ++n1)   // length-3 DFTs along n2
+  for (int a = 0; a < N2 * N3; ++a) {   // length-N1 DFTs along n1
+    const int k2 = a / N3, k3 = a % N3;
+    C v[N1];
 #pragma unroll
-    for (int k3 = 0; k3 < 5; ++k3) {
-      C v[3];
+    for (int r = 0; r < N1; ++r) v[r] = x[(Q1 * r + Q2 * k2 + Q3 * k3) % N];
+    dft_small<N1, INV>(v);
 #pragma unroll
-      for (int r = 0; r < 3; ++r) v[r] = y[(n1 * 3 + r) * 5 + k3];
-      dft_small<3, INV>(v);
-#pragma unroll
-      for (int r = 0; r < 3; ++r) y[(n1 * 3 + r) * 5 + k3] = v[r];
-    }
-#pragma unroll
-  for (int b = 0; b < 15; ++b) {   // length-2 DFTs along n1
-    C v[2] = {y[b], y[15 + b]};
-    dft_small<2, INV>(v);
-    y[b] = v[0];
-    y[15 + b] = v[1];
+    for (int r = 0; r < N1; ++r) x[(Q1 * r + Q2 * k2 + Q3 * k3) % N] = v[r];
   }
+  // result (k1, k2, k3) sits at input position (Q1 k1 + Q2 k2 + Q3 k3) % N and
+  // belongs at output position (M1 k1 + M2 k2 + M3 k3) % N
+  C y[N];
 #pragma unroll
-  for (int k1 = 0; k1 < 2; ++k1)
+  for (int k1 = 0; k1 < N1; ++k1)
 #pragma unroll
-    for (int k2 = 0; k2 < 3; ++k2)
+    for (int k2 = 0; k2 < N2; ++k2)
 #pragma unroll
-      for (int k3 = 0; k3 < 5; ++k3) x[(15 * k1 + 10 * k2 + 6 * k3) % 30] = y[(k1 * 3 + k2) * 5 + k3];
+      for (int k3 = 0; k3 < N3; ++k3) y[(M1 * k1 + M2 * k2 + M3 * k3) % N] = x[(Q1 * k1 + Q2 * k2 + Q3 * k3) % N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = y[i];
 }
 
 template <int N, bool INV, typename C>
 __device__ __forceinline__ void fft(C (&x)[N]) {
-  if constexpr (N == 30) fft30_pfa<INV>(x);
+  if constexpr (N == 30) fft_pfa3<2, 3, 5, INV>(x);
+  else if constexpr (N == 60) fft_pfa3<4, 3, 5, INV>(x);
   else fft_stages<N, 1, INV>(x);
 }
 

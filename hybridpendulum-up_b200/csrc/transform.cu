@@ -588,7 +588,8 @@ static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out,
 // pair: F^l_mn[w] = sum_b w_b d^l_mn(beta_b) Q_b[m][n][w], written straight
 // into the [row][omega] layout.  Every output has one owner: no atomics.
 template <int B, typename T, int PA, bool CPLX>
-__global__ void __launch_bounds__(256) k_anal_ag(const void* __restrict__ fin, const double* __restrict__ mult,
+__global__ void __launch_bounds__(B >= 24 ? 128 : 256, B >= 24 && sizeof(T) == 4 ? 3 : 1)
+    k_anal_ag(const void* __restrict__ fin, const double* __restrict__ mult,
                                                  c2<T>* __restrict__ Qg, long long w0, long long nwc) {
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
