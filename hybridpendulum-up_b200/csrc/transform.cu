@@ -429,8 +429,12 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
                               : (long long)p * 2 * B * rs * (long long)sizeof(T);
     return (GD ? 0 : nb * nrows * (long long)sizeof(T)) + 32 + (long long)NM * (2 * B - 1) * 8 + (g > st ? g : st);
   }
-  // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB)
-  static constexpr long long budget() { return bytes(1, 4) <= 110 * 1024 ? 110 * 1024 : 220 * 1024; }
+  // two resident blocks (110 KB each) when a batch of 4 fits, else one (220 KB);
+  // with the d table in global memory (large B) one block with two betas beat
+  // two blocks with one (B = 30, FP32: 10.2 vs 11.2 ms per launch at 60x60)
+  static constexpr long long budget() {
+    return (!GD && bytes(1, 4) <= 110 * 1024) ? 110 * 1024 : 220 * 1024;
+  }
   // betas per block: up to 4 (each coefficient then feeds 4 x P FMAs), as
   // many as keep a batch of 4 omega points within the budget
   static constexpr int pick_nb() {
