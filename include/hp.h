@@ -327,7 +327,10 @@ int hp_state_create(hp_plan* plan, hp_state** state);
 int hp_state_destroy(hp_state* state);
 int hp_state_load(hp_state* state, const double* F, int mem);   /* full layout in  */
 int hp_state_store(hp_state* state, double* F, int mem);        /* full layout out */
-/* nsteps steps of `method` with step dt. */
+/* nsteps steps of `method` with step dt.  Mixed-precision 3-D plans keep the
+ * coefficients also in FP32 between steps (read by the next step and by
+ * hp_state_density); the first call on such a state allocates those two
+ * buffers, so make it outside any CUDA stream capture. */
 int hp_state_step(hp_state* state, double dt, int method, int nsteps);
 /* nsteps hybrid steps of pendulum_reduced_hybrid.m:224-234, each
  *   F = propagate_den(F, f); f = fftSO3R backward(F); f += dt*df(f); F = forward(f)
