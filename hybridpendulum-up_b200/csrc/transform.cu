@@ -718,12 +718,24 @@ __global__ void __launch_bounds__(256) k_anal_beta(RowLayout L, const c2<T>* __r
 #pragma unroll
     for (int j = 0; j < B; ++j) {
       if (j < len) {
+        if constexpr (sizeof(T) == 4 && NB2 % 4 == 0) {
+          // four consecutive betas of one row in one 16-byte load (the row
+          // starts 16-byte aligned: NB2 and b0 are multiples of 4)
+          const float4 d4 = __ldg(reinterpret_cast<const float4*>(dsrc + (size_t)j * NB2 + b0));
+          const T dd[4] = {d4.x, d4.y, d4.z, d4.w};
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          if (b0 + u < NB2) {
-            const T d = __ldg(dsrc + (size_t)j * NB2 + b0 + u);
-            acc[j].x = fma(d, v[u].x, acc[j].x);
-            acc[j].y = fma(d, v[u].y, acc[j].y);
+          for (int u = 0; u < 4; ++u) {
+            acc[j].x = fma(dd[u], v[u].x, acc[j].x);
+            acc[j].y = fma(dd[u], v[u].y, acc[j].y);
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (b0 + u < NB2) {
+              const T d = __ldg(dsrc + (size_t)j * NB2 + b0 + u);
+              acc[j].x = fma(d, v[u].x, acc[j].x);
+              acc[j].y = fma(d, v[u].y, acc[j].y);
+            }
           }
         }
       }
