@@ -611,6 +611,30 @@ __global__ void __launch_bounds__(B >= 24 ? 128 : 256, B >= 24 && sizeof(T) == 4
   const int pc = (int)min((long long)PA, nwc - wl0);
   const int tid = threadIdx.x, nth = blockDim.x;
   const int NG = NB2 * NB2;
+  constexpr long long TILE = (long long)PA * (2LL * NM * NB2 > (long long)NB2 * NB2 * (CPLX ? 2 : 1)
+                                               ? 2LL * NM * NB2 : (long long)NB2 * NB2 * (CPLX ? 2 : 1));
+  T* smult = reinterpret_cast<T*>(smraw) + TILE;   // [c][a] multiplier of this beta (real densities)
+  // Real densities whose 2B-runs are 16-byte aligned: every run of 2B
+  // consecutive a arrives by 16-byte asynchronous copies (all in flight at
+  // once), the grid multiplier slice of this beta is staged beside it and
+  // applied when the alpha stage reads its lines.
+  constexpr bool ASYNC = !CPLX && (NB2 * sizeof(T)) % 16 == 0;
+  const bool async_ok = ASYNC && (reinterpret_cast<unsigned long long>(fin) & 15ull) == 0;
+  if (async_ok) {
+    constexpr int VPR = NB2 * (int)sizeof(T) / 16;                       // 16-byte pieces per run
+    for (int e = tid; e < pc * NB2 * VPR; e += nth) {
+      const int run = e / VPR, piece = e % VPR, pp = run / NB2, cc = run % NB2;
+      const long long w = w0 + wl0 + pp;
+      const long long gi = (long long)NB2 * ((long long)b + NB2 * ((long long)cc + NB2 * w));
+      cp_async<16>(sInR + (size_t)run * NB2 + piece * (16 / sizeof(T)),
+                   reinterpret_cast<const T*>(fin) + gi + piece * (16 / sizeof(T)), true);
+    }
+    for (int e = tid; e < NG; e += nth) {
+      const int cc = e / NB2, a = e % NB2;
+      smult[e] = mult ? (T)mult[a + NB2 * (b + NB2 * cc)] : (T)1;
+    }
+    cp_async_wait_all();
+  } else
   // load f(a, b, c, w) for this beta: runs of 2B consecutive a
   for (int e = tid; e < pc * NG; e += nth) {
     const int pp = e / NG, r = e % NG, cc = r / NB2, a = r % NB2;
@@ -642,6 +666,13 @@ __global__ void __launch_bounds__(B >= 24 ? 128 : 256, B >= 24 && sizeof(T) == 4
         const C* src = sIn + (size_t)tid * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) x[a] = src[a];
+      } else if (async_ok) {
+        const T* r0 = sInR + ((size_t)pp * NB2 + c0) * NB2;
+        const T* r1 = r0 + NB2;
+        const T* m0 = smult + (size_t)c0 * NB2;
+        const T* m1 = m0 + NB2;
+#pragma unroll
+        for (int a = 0; a < NB2; ++a) { x[a].x = r0[a] * m0[a]; x[a].y = r1[a] * m1[a]; }
       } else {
         const T* r0 = sInR + ((size_t)pp * NB2 + c0) * NB2;
         const T* r1 = r0 + NB2;
@@ -763,7 +794,11 @@ template <int B, typename T, bool CPLX> struct AnalCfg {
   static constexpr int NM = CPLX ? 2 * B - 1 : B;
   static constexpr long long in_w = (long long)(2 * B) * (2 * B) * (CPLX ? 2 : 1);   // T elements per omega
   static constexpr long long q_w = 2LL * NM * (2 * B);
-  static constexpr long long bytes(int pa) { return (long long)pa * (in_w > q_w ? in_w : q_w) * (long long)sizeof(T); }
+  // tiles for pa omega points, plus (real densities) this beta's grid multiplier slice
+  static constexpr long long bytes(int pa) {
+    return (long long)pa * (in_w > q_w ? in_w : q_w) * (long long)sizeof(T) +
+           (CPLX ? 0 : (long long)(2 * B) * (2 * B) * (long long)sizeof(T));
+  }
   static constexpr int items = CPLX ? 2 * B : B;    // alpha items per omega point
   // threads per block: from B = 24 the 2B-point register FFTs need ~170-255
   // registers, so two 128-thread blocks per SM overlap loads and FFTs
