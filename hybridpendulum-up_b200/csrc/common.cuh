@@ -103,6 +103,11 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool vali
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(nb) : "memory");
 }
+// the same with an explicit source byte count (0..BYTES; the rest zero-filled)
+__device__ __forceinline__ void cp_async16_n(void* smem, const void* gmem, int nbytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(nbytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }

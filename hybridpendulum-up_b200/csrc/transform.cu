@@ -145,10 +145,13 @@ __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
 // GD: the (2l+1) d table of the block's betas is read from a global table
 // [group][row][NB] (large bandlimits, where it does not fit shared memory)
 // instead of being staged from the d table `wig`.
-template <int B, typename T, int NB, int P, bool CPLX, bool GD>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout L, const c2<T>* __restrict__ Fp,
-                                                  const T* __restrict__ wig, const int2* __restrict__ pairs,
-                                                  void* __restrict__ fout, int nbatch) {
+// AF: the coefficients of each batch arrive in a shared-memory tile [row][P]
+// by cp.async issued during the previous batch's FFT and store stages, so the
+// beta contraction reads shared memory (512 threads, one block per SM).
+template <int B, typename T, int NB, int P, bool CPLX, bool GD, bool AF = false>
+__global__ void __launch_bounds__(AF ? 512 : 256, AF ? 1 : (sizeof(T) == 8 ? 1 : 2))
+    k_synth(RowLayout L, const c2<T>* __restrict__ Fp, const T* __restrict__ wig, const int2* __restrict__ pairs,
+            void* __restrict__ fout, int nbatch) {
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
   constexpr int NM = CPLX ? D : B;
@@ -168,7 +171,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   const int nrows = (int)L.nrows;
   T* sds = reinterpret_cast<T*>(smraw);
   int2* spairs = reinterpret_cast<int2*>(smraw + (GD ? 0 : ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16));
-  C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
+  C* scoef = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
+  C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(scoef) +
+                               (AF ? ((size_t)nrows * P * sizeof(C) + 15) / 16 * 16 : 0));
   // beta groups of one omega chunk are consecutive blocks, so they read the
   // same coefficient rows close together in time (L2 reuse)
   constexpr int NGROUPS = (NB2 + NB - 1) / NB;
@@ -187,10 +192,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
   const long long nx = L.nx;
   // vector and bulk stores need a 16-byte aligned density buffer
   const bool fout_al16 = (reinterpret_cast<unsigned long long>(fout) & 15ull) == 0;
+  // AF: rows of P omega points from w in 16-byte pieces; pieces past nx are
+  // (partly) zero-filled by the copy itself
+  constexpr int CPP = AF ? (int)(P * sizeof(C) / 16) : 1;   // pieces per row
+  auto coef_fetch = [&](long long w) {
+    for (int e = tid; e < nrows * CPP; e += nth) {
+      const int r = e / CPP, pc16 = e % CPP;
+      const long long wp = w + (long long)pc16 * (16 / (long long)sizeof(C));
+      const long long left = (nx - wp) * (long long)sizeof(C);
+      const int nb = left >= 16 ? 16 : (left > 0 ? (int)left : 0);
+      cp_async16_n(scoef + (size_t)r * P + pc16 * (16 / sizeof(C)), Fp + (size_t)r * nx + (nb ? wp : 0), nb);
+    }
+  };
+  if (AF && (long long)chunk * nbatch * P < nx) coef_fetch((long long)chunk * nbatch * P);
   for (int bt = 0; bt < nbatch; ++bt) {
     const long long w0 = ((long long)chunk * nbatch + bt) * P;
     if (w0 >= nx) break;
     if (BULK && fout_al16) bulk_wait_read_all();   // the previous batch's runs have left the staging (aliases sG)
+    if (AF) cp_async_wait_all();                   // this batch's coefficient tile
     __syncthreads();
     // beta stage: item (pair, p), p fastest.  Pairs come from the block's copy
     // of the pair table (longest l-runs first, so the lanes of a warp run
@@ -212,7 +231,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
           if (j0 < len) {
             C v[JB];
 #pragma unroll
-            for (int u = 0; u < JB; ++u) v[u] = (j0 + u < len) ? src[(size_t)(j0 + u) * nx] : czero<C>();
+            for (int u = 0; u < JB; ++u)
+              v[u] = (j0 + u < len) ? (AF ? scoef[(size_t)(s + j0 + u) * P + p] : src[(size_t)(j0 + u) * nx])
+                                    : czero<C>();
 #pragma unroll
             for (int u = 0; u < JB; ++u) {
               if (j0 + u < len) {
@@ -235,6 +256,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
       }
     }
     __syncthreads();
+    // the next batch's coefficients stream in while this one runs its FFT and store stages
+    if (AF && bt + 1 < nbatch && w0 + P < nx) coef_fetch(w0 + P);
     // gamma stage: item (bb, mi, p): FFT over n -> c, in place
     for (int it = tid; it < NB * NM * P; it += nth) {
       C* g = sG + (it / P) * GS + it % P;
@@ -346,6 +369,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2) k_synth(RowLayout
     }
   }
   if (BULK && fout_al16) bulk_wait_all();   // shared memory must outlive the bulk copies reading it
+  if (AF) cp_async_wait_all();
 }
 
 // -------------------------------------------------------------- drivers ----
@@ -448,6 +472,8 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
     return p;
   }
   static constexpr int P = pick_p();
+  // coefficient tile by cp.async (one 512-thread block per SM); off unless chosen below
+  static constexpr bool AF = false;
 };
 
 // (m, n) pairs with their row start, l-run length, m slot and n bin, longest
@@ -510,7 +536,9 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
                                         : (size_t)P * NB2 * RS * sizeof(T));
   constexpr int NPAIR = NM * (2 * B - 1);
   const size_t pr_bytes = ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16;
-  const size_t smem = sd_bytes + pr_bytes + sg_bytes;
+  constexpr bool AF = Cfg::AF;
+  const size_t cf_bytes = AF ? ((size_t)p->nrows * P * sizeof(C) + 15) / 16 * 16 : 0;
+  const size_t smem = sd_bytes + pr_bytes + cf_bytes + sg_bytes;
   if (smem > (size_t)smem_limit()) {
     hp_set_error("synthesis tables exceed shared memory for this bandlimit");
     return HP_ERR_UNSUPPORTED;
@@ -542,13 +570,13 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   }
   const long long nbatches = (p->nx + P - 1) / P;
   // about 8 resident waves of blocks over 148 SMs
-  long long gx = std::max(1LL, (148LL * 2 * 8) / ngroups);
+  long long gx = std::max(1LL, (148LL * (AF ? 1 : 2) * 8) / ngroups);
   int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
   gx = (nbatches + nbatch - 1) / nbatch;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX, GD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX, GD, AF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)(gx * ngroups), 1);
   ProfScope _ps(p, "tf.synth", s);
-  k_synth<B, T, NB, P, CPLX, GD><<<grid, 256, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
+  k_synth<B, T, NB, P, CPLX, GD, AF><<<grid, AF ? 512 : 256, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
