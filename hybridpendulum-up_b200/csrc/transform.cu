@@ -147,9 +147,10 @@ __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
 // instead of being staged from the d table `wig`.
 // AF: the coefficients of each batch arrive in a shared-memory tile [row][P]
 // by cp.async issued during the previous batch's FFT and store stages, so the
-// beta contraction reads shared memory (512 threads, one block per SM).
+// beta contraction reads shared memory (P >= 4: 512 threads, one block per SM;
+// P < 4: 256 threads, two blocks per SM).
 template <int B, typename T, int NB, int P, bool CPLX, bool GD, bool AF = false>
-__global__ void __launch_bounds__(AF ? 512 : 256, AF ? 1 : (sizeof(T) == 8 ? 1 : 2))
+__global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (sizeof(T) == 8 ? 1 : 2))
     k_synth(RowLayout L, const c2<T>* __restrict__ Fp, const T* __restrict__ wig, const int2* __restrict__ pairs,
             void* __restrict__ fout, int nbatch) {
   using C = c2<T>;
@@ -570,13 +571,14 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
   }
   const long long nbatches = (p->nx + P - 1) / P;
   // about 8 resident waves of blocks over 148 SMs
-  long long gx = std::max(1LL, (148LL * (AF ? 1 : 2) * 8) / ngroups);
+  constexpr int NT = AF && P >= 4 ? 512 : 256;
+  long long gx = std::max(1LL, (148LL * (NT == 512 ? 1 : 2) * 8) / ngroups);
   int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
   gx = (nbatches + nbatch - 1) / nbatch;
   HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX, GD, AF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)(gx * ngroups), 1);
   ProfScope _ps(p, "tf.synth", s);
-  k_synth<B, T, NB, P, CPLX, GD, AF><<<grid, AF ? 512 : 256, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
+  k_synth<B, T, NB, P, CPLX, GD, AF><<<grid, NT, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
