@@ -53,6 +53,8 @@ def parse():
                          'transform: B=32 round-trip precision stress; hybrid: the loop of '
                          'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega)')
     ap.add_argument('--members', type=int, default=64)
+    ap.add_argument('--beta-engine', default='auto', choices=['auto', 'simt', 'tensor'],
+                    help='forward-transform beta contraction (transform and hybrid workloads)')
     return ap.parse_args()
 
 
@@ -611,6 +613,7 @@ def bench_transform(args, rank, local):
     ns = (2 * B) ** 3 * N * N * 2            # first two omega planes of the density
     for name, prec in (('fp64', hp.HP_FP64), ('mixed', hp.HP_MIXED)):
         plan = hp.Plan(B, Bx, 3, prec, hp.HP_COMPLEX)
+        plan.set_beta_engine(beta_engine(hp, args))
         st = hp.State(plan)
         cdt = torch.complex128 if prec == hp.HP_FP64 else torch.complex64
         f = torch.empty((2 * B) ** 3 * N ** 3, dtype=cdt, device=dev)
@@ -647,12 +650,16 @@ def bench_transform(args, rank, local):
             'value': round(out['mixed']['backward_ms'] + out['mixed']['forward_ms'], 2), 'higher_is_better': False,
             'n_gpus': 1, 'dtype': 'f32 (mixed) and f64', 'data': 'synthetic',
             'config': {'workload': 'transform precision stress', 'B': B, 'omega_grid': '24^3',
-                       'coefficients': 'i.i.d. N(0,1)/(2l+1), complex'},
+                       'coefficients': 'i.i.d. N(0,1)/(2l+1), complex', 'beta_engine': args.beta_engine},
             'fp64': out['fp64'], 'mixed': out['mixed'],
             'not_built': 'TF32-split and BF16x3-split tensor-core beta contractions'}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def beta_engine(hp, args):
+    return {'auto': hp.HP_BETA_AUTO, 'simt': hp.HP_BETA_SIMT, 'tensor': hp.HP_BETA_TENSOR}[args.beta_engine]
 
 
 def bench_hybrid(args, rank, local):
@@ -683,6 +690,7 @@ def bench_hybrid(args, rank, local):
     out = {}
     for name, prec in (('mixed', hp.HP_MIXED), ('fp64', hp.HP_FP64)):
         plan = hp.Plan(B, Bx, 2, prec, hp.HP_REAL)
+        plan.set_beta_engine(beta_engine(hp, args))
         plan.set_den_model(L, b, G, mR)
         t0 = time.perf_counter()
         c = hp.Collision(plan, L=L, Gd=Gd, nD=10, **coll)
@@ -723,7 +731,7 @@ def bench_hybrid(args, rank, local):
             'value': out['mixed']['steps_per_s'], 'unit': 'steps/s', 'higher_is_better': True, 'n_gpus': 1,
             'steps': args.steps, 'warmup': args.warmup, 'dtype': 'f32 (f64 accumulation)', 'data': 'synthetic',
             'config': {'workload': 'hybrid loop body incl. get_stat moments', 'B': B, 'omega_grid': '60x60',
-                       'dt': dt, 'method': 'euler'},
+                       'dt': dt, 'method': 'euler', 'beta_engine': args.beta_engine},
             'mixed': out['mixed'], 'fp64': out['fp64'],
             'ER_max_abs_diff_mixed_vs_fp64': float(np.abs(er).max())}
     for k in ('mixed', 'fp64'):

@@ -31,6 +31,7 @@ HP_FP64, HP_MIXED = 0, 1
 HP_REAL, HP_COMPLEX = 0, 1
 HP_EULER, HP_MIDPOINT, HP_RK2, HP_RK4 = 0, 1, 2, 3
 HP_DEVICE, HP_HOST = 0, 1
+HP_BETA_AUTO, HP_BETA_SIMT, HP_BETA_TENSOR = 0, 1, 2
 METHODS = {'euler': HP_EULER, 'midpoint': HP_MIDPOINT, 'rk2': HP_RK2, 'rk4': HP_RK4}
 
 EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set_stream',
@@ -45,7 +46,7 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
            'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info',
            'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate', 'hp_fftSO3_real_forward',
-           'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod']
+           'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod', 'hp_plan_set_beta_engine', 'hp_plan_tc_errors']
 
 
 class HPError(RuntimeError):
@@ -147,6 +148,8 @@ def _load():
         'hp_fftSO3_real_forward': [vp, vp, vp, ip, ip],
         'hp_fftSO3_real_backward': [vp, vp, vp, ip, ip],
         'hp_fftSO3_real_prod': [vp, vp, vp, vp, ip, ip],
+        'hp_plan_set_beta_engine': [vp, ip],
+        'hp_plan_tc_errors': [vp, ctypes.POINTER(ip)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -279,6 +282,17 @@ class Plan:
             out[buf.value.decode()] = (ms.value, cnt.value)
             i += 1
         return out
+
+    def set_beta_engine(self, engine: int):
+        """Engine of the forward transform's beta contraction: HP_BETA_AUTO
+        (tensor cores in HP_MIXED plans), HP_BETA_SIMT or HP_BETA_TENSOR."""
+        _check(_lib.hp_plan_set_beta_engine(self._h, int(engine)))
+
+    def tc_errors(self) -> int:
+        """Tensor-core launches of this plan whose wait gave up (0 normally)."""
+        v = ctypes.c_int()
+        _check(_lib.hp_plan_tc_errors(self._h, ctypes.byref(v)))
+        return v.value
 
     def launch_count(self) -> int:
         v = ctypes.c_longlong()

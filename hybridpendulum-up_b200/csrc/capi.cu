@@ -120,6 +120,21 @@ extern "C" int hp_plan_launch_count(hp_plan* p, long long* count) {
   return HP_OK;
 }
 
+extern "C" int hp_plan_set_beta_engine(hp_plan* p, int engine) {
+  if (!p) { hp_set_error("null plan"); return HP_ERR_INVALID; }
+  if (engine != HP_BETA_AUTO && engine != HP_BETA_SIMT && engine != HP_BETA_TENSOR) {
+    hp_set_error("engine must be HP_BETA_AUTO, HP_BETA_SIMT or HP_BETA_TENSOR");
+    return HP_ERR_INVALID;
+  }
+  p->beta_engine = engine;
+  return HP_OK;
+}
+
+extern "C" int hp_plan_tc_errors(hp_plan* p, int* count) {
+  if (!p || !count) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  return hp::tc_beta_errors(p, count);
+}
+
 static bool valid_N(int N) {
   return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 30 || N == 32 || N == 40 ||
          N == 48 || N == 60;

@@ -65,6 +65,9 @@ struct hp_plan {
   double2* so3d64 = nullptr;
   float2* so3d32 = nullptr;
 
+  // engine of the forward transform's beta contraction (enum hp_beta_engine)
+  int beta_engine = 0;
+
   // profiling
   bool prof_on = false;
   std::vector<ProfEntry> prof;
@@ -156,6 +159,16 @@ int hp_backward_internal32(hp_plan* p, const float2* Fint32, void* f, int comple
 // [row][omega] coefficients in the plan's compute precision (c2<T>).
 int hp_forward_internal_T(hp_plan* p, const void* f, const double* mult, void* out, cudaStream_t s);
 int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s);
+namespace hp {
+// Tensor-core (tcgen05, TF32-split) beta contraction of the forward transform
+// (tc_beta.cu): FP32 plans with B <= 32.  Qg: stage-1 tiles of the omega chunk
+// [w0, w0 + nwc), stride nwc; out: [row][nx] FP32 coefficients.
+bool tc_beta_supported(const hp_plan* p);
+int tc_beta_forward(hp_plan* p, const float2* Qg, const int2* pairs, int npairs, float2* out, long long w0,
+                    long long nwc, cudaStream_t s);
+// number of launches whose wait on the tensor cores gave up (0 when none ran)
+int tc_beta_errors(hp_plan* p, int* count);
+}  // namespace hp
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s);
 int hp_forward_internal64(hp_plan* p, const double* f, double2* Fint, cudaStream_t s);
 // inverse (scaled 1/nx) / forward omega FFT of every row, in the plan's compute precision

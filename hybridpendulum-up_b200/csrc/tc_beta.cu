@@ -1,0 +1,371 @@
+// Beta contraction of the forward transform on the 5th-generation tensor cores
+// (tcgen05), FP32 plans.
+//
+// After the alpha/gamma stage (k_anal_ag) the forward transform of
+// fftSO3R.m:89-106 (MEX fftSO3R/kernel.cu:11-195) is, for each (m, n) pair, one
+// real GEMM over the quadrature nodes beta_b:
+//
+//   F^l_mn[w] = sum_b  w_b d^l_mn(beta_b) Q_b[m][n][w],   l = max(|m|,|n|)..lmax,
+//
+// with Q complex and w_b d real.  Here a CTA owns one pair and a run of omega
+// tiles; a tile is M = 128 real rows (64 complex omega points, real and
+// imaginary parts as separate rows), K = the 2B nodes (padded to a multiple of
+// 8), N = the pair's l values (padded to 16 or 32):
+//
+//   D[r][j] = sum_b A[r][b] W[j][b],   A[r][b] = (float view of Q_b)[r],  W = w_b d.
+//
+// Precision: FP32 through three TF32 products.  Each operand x is split into
+// hi = x rounded to TF32 (low 13 mantissa bits cleared) and lo = x - hi (exact
+// in FP32), and D accumulates A_hi W_hi + A_hi W_lo + A_lo W_hi in FP32 in
+// tensor memory; the dropped A_lo W_lo term and the tensor core's truncation of
+// lo are below 2^-21 relative per product.  W's split is taken from the FP64
+// table (lo = x64 - hi), so W carries ~34 significant bits.
+//
+// Shared-memory operands use the K-major, no-swizzle canonical layout: core
+// matrices of 8 rows x 16 bytes (4 TF32 values), the K chunks of one 8-row
+// group 128 bytes apart (leading byte offset) and the 8-row groups KP*32
+// bytes apart (stride byte offset).  One elected thread issues the MMAs and
+// commits them to an mbarrier; every warp then reads its 32 TMEM lanes
+// (tcgen05.ld 32x32b) and writes the rows straight into the [row][omega]
+// coefficient layout.
+#include <stdint.h>
+#include <algorithm>
+#include "common.cuh"
+#include "plan.hpp"
+
+namespace hp {
+namespace {
+
+__device__ __forceinline__ float tf32_rn(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, no swizzle, sm_100 version bits
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor of kind::tf32: F32 accumulator, TF32 A and B, both
+// K-major, no negation, N >> 3 at bit 17, M >> 4 at bit 24
+template <int M, int N> __host__ __device__ constexpr uint32_t idesc_tf32() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(done)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// bounded wait: gives up after ~2^31 SM cycles (about a second)
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(mbar, parity))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+constexpr int TC_M = 128;        // real rows per tile (64 complex omega points)
+constexpr int TC_TMEM_COLS = 32; // accumulator columns allocated (N <= 32)
+
+// Grid: (omega-tile runs, pairs).  Q: the stage-1 tiles as floats,
+// [(mi*2B + q)*2B + b][2*nwc]; tab: [row][2][KP] TF32 hi/lo of w_b d (zero for
+// b >= 2B); out: [row][nx] complex as floats.  err: set to 1 when a wait on the
+// tensor cores gives up.
+// STAGED: the raw tile [b][128 rows] of Q arrives in shared memory by 16-byte
+// cp.async copies issued while the previous tile's MMAs and epilogue run (the
+// whole tile in flight at once, no registers held); the split pass then reads
+// it from shared memory.  Requires nwc even (16-byte aligned rows).  Otherwise
+// each thread loads its row's values into registers, 32 at a time.
+template <int KP, int NP, bool STAGED>
+__global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, const float* __restrict__ tab,
+                                                 const int2* __restrict__ pairs, int NB2, long long nwc,
+                                                 int tiles_per_cta, float* __restrict__ out, long long nx,
+                                                 long long w0, int* __restrict__ err) {
+  static_assert(KP % 8 == 0 && KP <= 64, "K: multiple of 8, at most 64");
+  static_assert(NP == 16 || NP == 32, "N: 16 or 32");
+  constexpr int KC = KP / 4;                       // 16-byte K chunks per row
+  constexpr uint32_t LBO = 128, SBO = KC * 128;    // bytes
+  constexpr uint32_t A_BYTES = TC_M * KP * 4, B_BYTES = NP * KP * 4;
+  constexpr uint32_t S_BYTES = STAGED ? TC_M * KP * 4 : 0;
+  constexpr uint32_t IDESC = idesc_tf32<TC_M, NP>();
+  extern __shared__ __align__(1024) unsigned char tc_sm[];
+  unsigned char* sAh = tc_sm;
+  unsigned char* sAl = tc_sm + A_BYTES;
+  unsigned char* sBh = tc_sm + 2 * A_BYTES;
+  unsigned char* sBl = tc_sm + 2 * A_BYTES + B_BYTES;
+  float* sS = reinterpret_cast<float*>(tc_sm + 2 * A_BYTES + 2 * B_BYTES);   // raw tile [KP][128]
+  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(tc_sm + 2 * A_BYTES + 2 * B_BYTES + S_BYTES);
+  uint32_t* tmem_p = reinterpret_cast<uint32_t*>(mbar_p + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int2 pe = pairs[blockIdx.y];
+  const int s = pe.x, len = pe.y & 0xff, mi = (pe.y >> 8) & 0xff, q = (pe.y >> 16) & 0xff;
+  const uint32_t mbar = smem_u32(mbar_p);
+  const float* Qp = Q + (size_t)(mi * NB2 + q) * NB2 * 2 * nwc;
+  const long long ntiles = (nwc + TC_M / 2 - 1) / (TC_M / 2);
+  const long long t_begin = (long long)blockIdx.x * tiles_per_cta;
+  const long long t_end = t_begin + tiles_per_cta < ntiles ? t_begin + tiles_per_cta : ntiles;
+  // raw tile t: row b < NB2 of Q in 32 pieces of 16 bytes; pieces past the
+  // chunk's 2*nwc real rows are zero-filled by the copy itself
+  auto stage = [&](long long t) {
+    const long long r0 = t * TC_M;
+    for (int e = tid; e < NB2 * 32; e += 128) {
+      const int b = e >> 5, pc = e & 31;
+      const long long r = r0 + pc * 4;
+      const bool in = r < 2 * nwc;
+      cp_async16_n(sS + b * TC_M + pc * 4, Qp + (size_t)b * 2 * nwc + (in ? r : 0), in ? 16 : 0);
+    }
+  };
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_p)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) mbar_init(mbar, 1);
+  if (STAGED) {
+    for (int e = tid; e < (KP - NB2) * TC_M; e += 128) sS[NB2 * TC_M + e] = 0.f;   // K padding rows
+    if (t_begin < t_end) stage(t_begin);
+  }
+  // W tile (hi, lo): item (j, K chunk), rows j >= len zero
+  for (int it = tid; it < NP * KC; it += 128) {
+    const int j = it / KC, kc = it % KC;
+    float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+    if (j < len) {
+      const float* rowp = tab + (size_t)(s + j) * 2 * KP + kc * 4;
+      h = *reinterpret_cast<const float4*>(rowp);
+      l = *reinterpret_cast<const float4*>(rowp + KP);
+    }
+    const uint32_t off = (j >> 3) * SBO + kc * 128 + (j & 7) * 16;
+    *reinterpret_cast<float4*>(sBh + off) = h;
+    *reinterpret_cast<float4*>(sBl + off) = l;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_p;
+
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint32_t aoff = (tid >> 3) * SBO + (tid & 7) * 16;   // this thread's row r = tid
+  for (long long t = t_begin; t < t_end && ok; ++t) {
+    const long long r0 = t * TC_M;                          // first real row of the tile
+    const long long rows = 2 * nwc - r0 < TC_M ? 2 * nwc - r0 : TC_M;
+    const bool rv = tid < rows;
+    if (STAGED) {
+      cp_async_wait_all();
+      __syncthreads();                                      // tile t is in sS
+#pragma unroll
+      for (int kc = 0; kc < KC; ++kc) {
+        float x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = sS[(kc * 4 + u) * TC_M + tid];
+        float4 h, l;
+        h.x = tf32_rn(x[0]); l.x = x[0] - h.x;
+        h.y = tf32_rn(x[1]); l.y = x[1] - h.y;
+        h.z = tf32_rn(x[2]); l.z = x[2] - h.z;
+        h.w = tf32_rn(x[3]); l.w = x[3] - h.w;
+        *reinterpret_cast<float4*>(sAh + aoff + kc * 128) = h;
+        *reinterpret_cast<float4*>(sAl + aoff + kc * 128) = l;
+      }
+    } else {
+      // A tile: row r = tid, all K chunks; 8 chunks (32 loads) in flight at a time
+#pragma unroll
+      for (int k0 = 0; k0 < KC; k0 += 8) {
+        float v[8][4];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int b = (k0 + c) * 4 + u;
+            v[c][u] = (k0 + c < KC && rv && b < NB2) ? __ldg(Qp + (size_t)b * 2 * nwc + r0 + tid) : 0.f;
+          }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          if (k0 + c < KC) {
+            float4 h, l;
+            h.x = tf32_rn(v[c][0]); l.x = v[c][0] - h.x;
+            h.y = tf32_rn(v[c][1]); l.y = v[c][1] - h.y;
+            h.z = tf32_rn(v[c][2]); l.z = v[c][2] - h.z;
+            h.w = tf32_rn(v[c][3]); l.w = v[c][3] - h.w;
+            *reinterpret_cast<float4*>(sAh + aoff + (k0 + c) * 128) = h;
+            *reinterpret_cast<float4*>(sAl + aoff + (k0 + c) * 128) = l;
+          }
+        }
+      }
+    }
+    fence_async_smem();   // generic-proxy smem writes -> visible to the tensor core
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      const uint32_t ah = smem_u32(sAh), al = smem_u32(sAl), bh = smem_u32(sBh), bl = smem_u32(sBl);
+#pragma unroll
+      for (int kk = 0; kk < KP / 8; ++kk) {
+        const uint32_t o = kk * 2 * 128;
+        umma_tf32(tmem, umma_desc(ah + o, LBO, SBO), umma_desc(bh + o, LBO, SBO), IDESC, kk > 0 ? 1u : 0u);
+        umma_tf32(tmem, umma_desc(ah + o, LBO, SBO), umma_desc(bl + o, LBO, SBO), IDESC, 1u);
+        umma_tf32(tmem, umma_desc(al + o, LBO, SBO), umma_desc(bh + o, LBO, SBO), IDESC, 1u);
+      }
+      umma_commit(mbar);
+    }
+    // the raw tile was consumed before the barrier: the next one streams in
+    // while the tensor core and the epilogue work on this one
+    if (STAGED && t + 1 < t_end) stage(t + 1);
+    // every thread takes the same branch (a wait that gave up anywhere ends the block's loop)
+    ok = __syncthreads_and(mbar_wait(mbar, phase)) != 0;
+    phase ^= 1u;
+    if (!ok) {
+      if (lane == 0) atomicExch(err, 1);
+      break;
+    }
+    tc_fence_after();
+    // epilogue: warp w reads TMEM lanes 32w..32w+31 = rows r0 + 32w + lane
+    float* orow = out + ((size_t)s * nx + w0) * 2 + r0 + tid;
+#pragma unroll
+    for (int c0 = 0; c0 < NP; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (rv && c0 + j < len) orow[(size_t)(c0 + j) * nx * 2] = v[j];
+    }
+    tc_fence_before();
+    __syncthreads();      // every TMEM read done before the next tile's MMAs overwrite D
+    tc_fence_after();
+  }
+  if (!ok) {
+    // the tensor core did not signal: wait once more (bounded) before
+    // releasing the accumulator it may still be writing
+    mbar_wait(mbar, phase ^ 1u);
+  }
+  if (STAGED) cp_async_wait_all();   // no copy into this block's shared memory outlives it
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
+                 : "memory");
+}
+
+// [row][2][KP]: TF32 hi and lo parts of w_b d^l_mn(beta_b), from FP64
+__global__ void k_dwtc_table(RowLayout L, const double* __restrict__ wig, const double* __restrict__ qw, int KP,
+                             float* __restrict__ tab) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * KP) return;
+  const long long r = t / KP;
+  const int b = (int)(t % KP);
+  const int NB2 = 2 * L.B;
+  const double x = b < NB2 ? qw[b] * wig[(size_t)b * L.nrows + r] : 0.0;
+  const float hi = tf32_rn((float)x);
+  tab[(r * 2) * KP + b] = hi;
+  tab[(r * 2 + 1) * KP + b] = (float)(x - (double)hi);
+}
+
+template <int KP, int NP>
+int tc_launch(hp_plan* p, const float2* Qg, const float* tab, const int2* pairs, int npairs, float2* out,
+              long long w0, long long nwc, int* err, cudaStream_t s) {
+  const bool staged = nwc % 2 == 0;
+  const size_t smem = 2 * (size_t)TC_M * KP * 4 + 2 * (size_t)NP * KP * 4 + (staged ? (size_t)TC_M * KP * 4 : 0) + 16;
+  auto kern = staged ? k_tc_beta<KP, NP, true> : k_tc_beta<KP, NP, false>;
+  HP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long ntiles = (nwc + TC_M / 2 - 1) / (TC_M / 2);
+  // about 16 waves of CTAs over 148 SMs, at least 2 tiles per CTA
+  long long per = std::max(2LL, (ntiles * npairs + 148LL * 4 * 16 - 1) / (148LL * 4 * 16));
+  per = std::min(per, ntiles);
+  const dim3 grid((unsigned)((ntiles + per - 1) / per), (unsigned)npairs);
+  kern<<<grid, 128, smem, s>>>(reinterpret_cast<const float*>(Qg), tab, pairs, 2 * p->B, nwc,
+                                            (int)per, reinterpret_cast<float*>(out), p->nx, w0, err);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+}  // namespace
+
+bool tc_beta_supported(const hp_plan* p) { return p->precision == HP_MIXED && p->B >= 2 && p->B <= 32; }
+
+int tc_beta_forward(hp_plan* p, const float2* Qg, const int2* pairs, int npairs, float2* out, long long w0,
+                    long long nwc, cudaStream_t s) {
+  if (!tc_beta_supported(p)) {
+    hp_set_error("tensor-core beta contraction: FP32 plans with B <= 32 only");
+    return HP_ERR_UNSUPPORTED;
+  }
+  const int KP = (2 * p->B + 7) / 8 * 8;
+  int st = HP_OK;
+  bool have = false;
+  for (auto& kv : p->ws) if (kv.first == "tf.dwtc") have = true;
+  float* tab = (float*)p->ws_get("tf.dwtc", sizeof(float) * 2 * (size_t)p->nrows * KP, &st);
+  if (st) return st;
+  int* err = (int*)p->ws_get("tf.tcerr", sizeof(int), &st);
+  if (st) return st;
+  if (!have) {
+    HP_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+    const long long n = p->nrows * KP;
+    k_dwtc_table<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), p->wig64, p->qw, KP, tab);
+    HP_CUDA_TRY(cudaGetLastError());
+  }
+  ProfScope _ps(p, "tf.anal.beta.tc", s);
+  const bool n16 = p->B <= 16;
+  switch (KP) {
+    case 8: return n16 ? tc_launch<8, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s)
+                       : tc_launch<8, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 16: return tc_launch<16, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 24: return tc_launch<24, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 32: return tc_launch<32, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 40: return tc_launch<40, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 48: return tc_launch<48, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 64: return tc_launch<64, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    default:
+      hp_set_error("tensor-core beta contraction: unsupported node count");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
+int tc_beta_errors(hp_plan* p, int* count) {
+  *count = 0;
+  for (auto& kv : p->ws)
+    if (kv.first == "tf.tcerr") {
+      HP_CUDA_TRY(cudaMemcpy(count, kv.second.p, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+  return HP_OK;
+}
+
+}  // namespace hp

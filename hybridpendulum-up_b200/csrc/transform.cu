@@ -888,6 +888,14 @@ static int anal2_launch(hp_plan* p, const void* f, const double* mult, c2<T>* ou
       k_anal_ag<B, T, PA, CPLX><<<ga, Cfg::NT, smem, s>>>(f, mult, Qg, w0, nw);
       HP_CUDA_TRY(cudaGetLastError());
     }
+    if constexpr (sizeof(T) == 4) {
+      if (p->beta_engine != HP_BETA_SIMT && tc_beta_supported(p)) {
+        st = tc_beta_forward(p, reinterpret_cast<const float2*>(Qg), dpairs, NPAIR, reinterpret_cast<float2*>(out),
+                             w0, nw, s);
+        if (st) return st;
+        continue;
+      }
+    }
     ProfScope _ps(p, "tf.anal.beta", s);
     dim3 gb((unsigned)((nw + 31) / 32), (unsigned)((NPAIR + 7) / 8));
     k_anal_beta<B, T, CPLX><<<gb, 256, 0, s>>>(p->layout(), Qg, dw, dpairs, NPAIR, out, w0, nw);

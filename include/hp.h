@@ -102,6 +102,18 @@ int hp_plan_profile_get(hp_plan* plan, int i, char* name, int name_cap, double* 
                         long long* count);
 int hp_plan_launch_count(hp_plan* plan, long long* count);
 
+/* Engine of the forward transform's beta contraction, the stage
+ * F^l_mn[w] = sum_b w_b d^l_mn(beta_b) Q_b[m][n][w] of fftSO3R.m:89-106 (the
+ * per-degree cuTENSOR contractions of the MEX, fftSO3R/kernel.cu:130-180).
+ * HP_BETA_AUTO: the tensor cores (tcgen05, three TF32 products per FP32
+ * product) in HP_MIXED plans, FP64 SIMT in HP_FP64 plans; HP_BETA_SIMT: FP32 or
+ * FP64 CUDA-core FMAs; HP_BETA_TENSOR: as AUTO.  hp_plan_tc_errors returns how
+ * many tensor-core launches of the plan had a wait give up (their outputs are
+ * not valid; 0 in normal operation; reading it synchronises the device). */
+enum hp_beta_engine { HP_BETA_AUTO = 0, HP_BETA_SIMT = 1, HP_BETA_TENSOR = 2 };
+int hp_plan_set_beta_engine(hp_plan* plan, int engine);
+int hp_plan_tc_errors(hp_plan* plan, int* count);
+
 /* Model for the propagation entry points.  MR: complex (2lmax+1,2lmax+1,lmax+1,ndim)
  * in the full layout; only its degree-1, m2=0 block may be non-zero (the
  * gravity term of pendulum.m:166-192 depends on R through R^T e3 only);
