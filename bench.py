@@ -652,7 +652,9 @@ def bench_transform(args, rank, local):
             'config': {'workload': 'transform precision stress', 'B': B, 'omega_grid': '24^3',
                        'coefficients': 'i.i.d. N(0,1)/(2l+1), complex', 'beta_engine': args.beta_engine},
             'fp64': out['fp64'], 'mixed': out['mixed'],
-            'not_built': 'TF32-split and BF16x3-split tensor-core beta contractions'}
+            'beta_contraction': {'forward': 'tcgen05 tensor cores, 3xTF32 split (mixed; --beta-engine simt: CUDA cores)',
+                                 'backward': 'CUDA cores, fused with the gamma/alpha FFTs'},
+            'not_built': 'BF16x3-split beta contraction'}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
