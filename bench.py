@@ -48,10 +48,11 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--fp64-steps', type=int, default=None)
-    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform', 'hybrid'],
+    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform', 'hybrid', 'forward'],
                     help='step: the headline FP step; batch: uneven-bandlimit batch of densities; '
                          'transform: B=32 round-trip precision stress; hybrid: the loop of '
-                         'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega)')
+                         'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega); '
+                         'forward: one FP32 forward transform on a 2-D omega grid (--B, --Bx, --beta-engine)')
     ap.add_argument('--members', type=int, default=64)
     ap.add_argument('--beta-engine', default='auto', choices=['auto', 'simt', 'tensor'],
                     help='forward-transform beta contraction (transform and hybrid workloads)')
@@ -280,6 +281,8 @@ def main():
         return bench_transform(args, rank, local)
     if args.workload == 'hybrid':
         return bench_hybrid(args, rank, local)
+    if args.workload == 'forward':
+        return bench_forward(args, rank, local)
     if args.impl == 'reference':
         if rank != 0:
             return 0
@@ -655,6 +658,47 @@ def bench_transform(args, rank, local):
             'beta_contraction': {'forward': 'tcgen05 tensor cores, 3xTF32 split (mixed; --beta-engine simt: CUDA cores)',
                                  'backward': 'CUDA cores, fused with the gamma/alpha FFTs'},
             'not_built': 'BF16x3-split beta contraction'}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_forward(args, rank, local):
+    """One forward transform (fftSO3R) of a random FP32 density on a 2-D omega
+    grid, B = --B, 2Bx = 2 * --Bx, mixed plan, through the state API
+    (hp_state_load_density): the small case the beta-contraction profiles are
+    captured on.  Prints one JSON line (not the headline)."""
+    import torch
+    torch.cuda.set_device(local)
+    hp = importlib.import_module('hybridpendulum-up_b200')
+    B, Bx = args.B, args.Bx
+    plan = hp.Plan(B, Bx, 2, hp.HP_MIXED, hp.HP_REAL)
+    plan.set_beta_engine(beta_engine(hp, args))
+    g = torch.Generator(device='cuda').manual_seed(11 + rank)
+    f = torch.rand((2 * B) ** 3 * (2 * Bx) ** 2, dtype=torch.float32, device='cuda', generator=g)
+    st = hp.State(plan)
+    for _ in range(max(args.warmup, 1)):
+        st.load_density(f.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        st.load_density(f.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    plan.profile(True)
+    for _ in range(2):
+        st.load_density(f.data_ptr())
+    torch.cuda.synchronize()
+    fam = {k: round(v[0] / v[1], 4) for k, v in plan.profile_read().items()}
+    plan.profile(False)
+    line = {'metric': f'fftSO3R forward, B={B}, omega {2 * Bx}x{2 * Bx}, FP32 plan', 'value': round(ms, 4),
+            'unit': 'ms', 'higher_is_better': False, 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
+            'dtype': 'f32', 'data': 'synthetic (uniform random density)',
+            'config': {'workload': 'forward transform', 'B': B, 'omega_grid': f'{2 * Bx}x{2 * Bx}',
+                       'beta_engine': args.beta_engine},
+            'kernel_ms_per_launch': fam, 'tc_errors': plan.tc_errors()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
