@@ -38,6 +38,9 @@ def test_argument_validation_without_gpu(hp):
     assert lib.hp_plan_destroy(None) == hp.HP_OK
     assert lib.hp_state_step(None, ctypes.c_double(1e-3), 0, 1) == hp.HP_ERR_INVALID
     assert lib.hp_pendulum_propagate(None, None, None, ctypes.c_double(1e-3), 0, 0) == hp.HP_ERR_INVALID
+    assert lib.hp_plan_set_beta_engine(None, hp.HP_BETA_TENSOR) == hp.HP_ERR_INVALID
+    cnt = ctypes.c_int(-1)
+    assert lib.hp_plan_tc_errors(None, ctypes.byref(cnt)) == hp.HP_ERR_INVALID
 
 
 def test_plan_creation_fails_cleanly_without_device(hp):
