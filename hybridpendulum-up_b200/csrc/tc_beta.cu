@@ -24,8 +24,8 @@
 // Shared-memory operands use the K-major, no-swizzle canonical layout: core
 // matrices of 8 rows x 16 bytes (4 TF32 values), the K chunks of one 8-row
 // group 128 bytes apart (leading byte offset) and the 8-row groups KP*32
-// bytes apart (stride byte offset).  One elected thread issues the MMAs and
-// commits them to an mbarrier; every warp then reads its 32 TMEM lanes
+// bytes apart (stride byte offset).  One thread issues the MMAs and commits
+// them to an mbarrier; every warp then reads its 32 TMEM lanes
 // (tcgen05.ld 32x32b) and writes the rows straight into the [row][omega]
 // coefficient layout.
 #include <stdint.h>
@@ -312,8 +312,8 @@ int tc_launch(hp_plan* p, const float2* Qg, const float* tab, const int2* pairs,
   long long per = std::max(2LL, (ntiles * npairs + 148LL * 4 * 16 - 1) / (148LL * 4 * 16));
   per = std::min(per, ntiles);
   const dim3 grid((unsigned)((ntiles + per - 1) / per), (unsigned)npairs);
-  kern<<<grid, 128, smem, s>>>(reinterpret_cast<const float*>(Qg), tab, pairs, 2 * p->B, nwc,
-                                            (int)per, reinterpret_cast<float*>(out), p->nx, w0, err);
+  kern<<<grid, 128, smem, s>>>(reinterpret_cast<const float*>(Qg), tab, pairs, 2 * p->B, nwc, (int)per,
+                               reinterpret_cast<float*>(out), p->nx, w0, err);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }
