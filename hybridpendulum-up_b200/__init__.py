@@ -285,7 +285,8 @@ class Plan:
 
     def set_beta_engine(self, engine: int):
         """Engine of the forward transform's beta contraction: HP_BETA_AUTO
-        (tensor cores in HP_MIXED plans), HP_BETA_SIMT or HP_BETA_TENSOR."""
+        (tensor cores in HP_MIXED plans with B >= 15), HP_BETA_SIMT or
+        HP_BETA_TENSOR (tensor cores in every HP_MIXED plan)."""
         _check(_lib.hp_plan_set_beta_engine(self._h, int(engine)))
 
     def tc_errors(self) -> int:

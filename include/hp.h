@@ -106,8 +106,9 @@ int hp_plan_launch_count(hp_plan* plan, long long* count);
  * F^l_mn[w] = sum_b w_b d^l_mn(beta_b) Q_b[m][n][w] of fftSO3R.m:89-106 (the
  * per-degree cuTENSOR contractions of the MEX, fftSO3R/kernel.cu:130-180).
  * HP_BETA_AUTO: the tensor cores (tcgen05, three TF32 products per FP32
- * product) in HP_MIXED plans, FP64 SIMT in HP_FP64 plans; HP_BETA_SIMT: FP32 or
- * FP64 CUDA-core FMAs; HP_BETA_TENSOR: as AUTO.  hp_plan_tc_errors returns how
+ * product) in HP_MIXED plans with B >= 15, CUDA-core FMAs otherwise (FP64
+ * plans always); HP_BETA_SIMT: CUDA-core FMAs; HP_BETA_TENSOR: the tensor cores
+ * in every HP_MIXED plan.  hp_plan_tc_errors returns how
  * many tensor-core launches of the plan had a wait give up (their outputs are
  * not valid; 0 in normal operation; reading it synchronises the device). */
 enum hp_beta_engine { HP_BETA_AUTO = 0, HP_BETA_SIMT = 1, HP_BETA_TENSOR = 2 };

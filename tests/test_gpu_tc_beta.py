@@ -68,7 +68,7 @@ def test_tc_beta_many_tiles(hp, B, Bx, ndim):
 
 
 def test_tc_beta_default_engine(hp):
-    # HP_MIXED plans take the tensor-core contraction unless told otherwise
+    # HP_MIXED plans with B >= 15 take the tensor-core contraction unless told otherwise
     B, Bx = 15, 2
     F = coeffs(B, (4, 4), 3, True)
     plan = hp.Plan(B, Bx, 2, hp.HP_MIXED, hp.HP_REAL)
