@@ -112,8 +112,11 @@ constexpr int TC_TMEM_COLS = 32; // accumulator columns allocated (N <= 32)
 // STAGED: the raw tile [b][128 rows] of Q arrives in shared memory by 16-byte
 // cp.async copies issued while the previous tile's MMAs and epilogue run (the
 // whole tile in flight at once, no registers held); the split pass then reads
-// it from shared memory.  Requires nwc even (16-byte aligned rows).  Otherwise
-// each thread loads its row's values into registers, 32 at a time.
+// it from shared memory.  Requires nwc even (16-byte aligned rows), which every
+// omega chunk of a plan satisfies (nx = (2Bx)^ndim is even and full chunks are
+// multiples of 32 points); for an odd chunk length the kernel instead loads
+// each row's values into registers, 32 at a time (the GPU tests run only the
+// staged form, since no plan produces an odd chunk).
 template <int KP, int NP, bool STAGED>
 __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, const float* __restrict__ tab,
                                                  const int2* __restrict__ pairs, int NB2, long long nwc,
