@@ -375,6 +375,60 @@ def derivative_fast(F: np.ndarray, P: Pendulum, *, gravity: str = 'l2=1') -> np.
     return dF
 
 
+def derivative_fast_mgroup(Fm: np.ndarray, m: int, P: Pendulum) -> np.ndarray:
+    """The rows of one order m of ``derivative_fast``, from the rows of that m alone.
+
+    Every term of the pendulum derivative keeps m (the alpha frequency):
+    the Lie matrices u^l_i act on n by right multiplication (pendulum.m:418-420,
+    getu.m:132-163); damping, gyroscopic and noise terms are pointwise in
+    (l, m, n) (pendulum.m:424-466, 510-523); and the gravity multiplier
+    mR_i(R) = sum_j A_ij R_3j depends on R only through its third row
+    (-sin b cos g, sin b sin g, cos b), which does not involve alpha, so MR^1 is
+    non-zero only at m2 = 0 and the l2 = 1 product of pendulum.m:474-502 keeps m.
+    This lets the full-size workload (B = 15 on a 32^3 omega grid, 6.6 GB per
+    full coefficient array) be checked one m group at a time.
+    Fm = F[m + lmax] (shape (2lmax+1, lmax+1, *x)); returns dF[m + lmax]."""
+    lmax, Bx, L, nd = P.lmax, P.Bx, P.L, P.ndim
+    N = 2 * Bx
+    ax = tuple(range(2, 2 + nd))
+    u = so3.getu(lmax)
+    MR1 = [P.MR[lmax - 1:lmax + 2, lmax - 1:lmax + 2, 1, i] for i in range(nd)]
+    for blk in MR1:
+        scale = max(np.abs(blk).max(), 1e-300)
+        if max(np.abs(blk[0]).max(), np.abs(blk[2]).max()) > 1e-12 * scale:
+            raise ValueError('gravity multiplier depends on alpha: m groups are coupled')
+    Fp = sfft.ifftn(Fm, axes=ax)
+    xs = [sfft.ifftn(P.X[..., i]) for i in range(nd)]
+    PF = [sfft.fftn(Fp * xs[i], axes=ax) for i in range(nd)]
+    dF = np.zeros_like(Fm)
+    for l in range(abs(m), lmax + 1):
+        s = slice(lmax - l, lmax + l + 1)
+        for i in range(nd):
+            blk = np.moveaxis(PF[i][s, l], 0, -1)                  # (*x, n)
+            dF[s, l] -= np.moveaxis(blk @ u[s, s, l, i].T, -1, 0)
+    c = _c_first(Bx, L)
+
+    def cmul(T, i):
+        sh = [1] * (2 + nd)
+        sh[2 + i] = N
+        return T * c.reshape(sh)
+
+    for i in range(nd):
+        dF -= cmul(-P.b[i] * PF[i], i)
+    if nd == 3 and P.OJO is not None:
+        for i in range(3):
+            ojo = sfft.ifftn(P.OJO[..., i])
+            dF -= cmul(sfft.fftn(Fp * ojo, axes=ax), i)
+    for i in range(nd):
+        g = np.zeros_like(Fm)
+        for (l, mm, n, l1, m1, n1, w) in gravity_taps(lmax, MR1[i]):
+            if mm == m and m1 == m:
+                g[n + lmax, l] += w * Fm[n1 + lmax, l1]
+        dF -= cmul(g, i)
+    dF += Fm * _noise_mult(Bx, L, nd, P.G)
+    return dF
+
+
 def integrate(F: np.ndarray, deriv, dt: float, method: str = 'euler') -> np.ndarray:
     """Time integrators of pendulum.m:346-385 (euler, midpoint, RK2, RK4)."""
     method = method.lower()
