@@ -26,12 +26,12 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, 'libhp.so')
 
 HP_OK, HP_ERR_INVALID, HP_ERR_SHAPE, HP_ERR_ALLOC, HP_ERR_CUDA = 0, 1, 2, 3, 4
-HP_ERR_UNSUPPORTED, HP_ERR_NONFINITE, HP_ERR_NO_MODEL = 5, 6, 7
+HP_ERR_UNSUPPORTED, HP_ERR_NONFINITE, HP_ERR_NO_MODEL, HP_ERR_MASS_DRIFT = 5, 6, 7, 8
 HP_FP64, HP_MIXED = 0, 1
 HP_REAL, HP_COMPLEX = 0, 1
 HP_EULER, HP_MIDPOINT, HP_RK2, HP_RK4 = 0, 1, 2, 3
 HP_DEVICE, HP_HOST = 0, 1
-HP_BETA_AUTO, HP_BETA_SIMT, HP_BETA_TENSOR = 0, 1, 2
+HP_BETA_AUTO, HP_BETA_SIMT, HP_BETA_TENSOR, HP_BETA_TENSOR_BF16 = 0, 1, 2, 3
 METHODS = {'euler': HP_EULER, 'midpoint': HP_MIDPOINT, 'rk2': HP_RK2, 'rk4': HP_RK4}
 
 EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set_stream',
@@ -46,7 +46,9 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_pendulum_adjoint', 'hp_moments', 'hp_state_moments', 'hp_density_mf_gauss',
            'hp_state_init_mf_gauss', 'hp_state_load_density', 'hp_batch_create', 'hp_batch_destroy', 'hp_batch_step', 'hp_batch_info',
            'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate', 'hp_fftSO3_real_forward',
-           'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod', 'hp_plan_set_beta_engine', 'hp_plan_tc_errors']
+           'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod', 'hp_plan_set_beta_engine', 'hp_plan_tc_errors',
+           'hp_collision_lambda', 'hp_collision_omega', 'hp_collision_fcL', 'hp_collision_create_from_tables',
+           'hp_state_set_guard', 'hp_set_device_budget', 'hp_device_bytes']
 
 
 class HPError(RuntimeError):
@@ -150,6 +152,13 @@ def _load():
         'hp_fftSO3_real_prod': [vp, vp, vp, vp, ip, ip],
         'hp_plan_set_beta_engine': [vp, ip],
         'hp_plan_tc_errors': [vp, ctypes.POINTER(ip)],
+        'hp_collision_lambda': [vp, ctypes.POINTER(hp_collision_params), ctypes.POINTER(ip), vp, vp, vp, ip],
+        'hp_collision_omega': [vp, ctypes.POINTER(hp_collision_params), ip, vp, vp, ip],
+        'hp_collision_fcL': [vp, ctypes.POINTER(hp_collision_params), ip, vp, vp, vp, vp, ip],
+        'hp_collision_create_from_tables': [vp, ip, ip, vp, vp, vp, vp, ip, ctypes.POINTER(vp)],
+        'hp_state_set_guard': [vp, ip, dp],
+        'hp_set_device_budget': [ctypes.c_longlong],
+        'hp_device_bytes': [ctypes.POINTER(ctypes.c_longlong)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -579,6 +588,24 @@ class State:
         _check(_lib.hp_state_mass(self._h, ctypes.byref(v)))
         return v.value
 
+    def set_guard(self, check_every: int = 1, mass_rtol: float = 0.0):
+        """Health check every check_every steps: NaN/Inf in the coefficients
+        (HP_ERR_NONFINITE) and, with mass_rtol > 0, l = 0 mass drift from its
+        value now (HP_ERR_MASS_DRIFT).  check_every = 0 turns it off."""
+        _check(_lib.hp_state_set_guard(self._h, int(check_every), float(mass_rtol)))
+
+
+def set_device_budget(nbytes: int):
+    """Cap the device bytes the library may hold at once (0: no cap)."""
+    _check(_lib.hp_set_device_budget(int(nbytes)))
+
+
+def device_bytes() -> int:
+    """Device bytes the library holds now."""
+    v = ctypes.c_longlong()
+    _check(_lib.hp_device_bytes(ctypes.byref(v)))
+    return v.value
+
 
 # ---------------------------------------------------------------- helpers ----
 def _as_matlab(a, dtype):
@@ -604,16 +631,29 @@ class Collision:
     operator on a 3-D Omega grid (Gd then 3x3)."""
 
     def __init__(self, plan: Plan, d, h, r, theta_t, lambda_max, epsilon, L, Gd, nD=10):
-        p = hp_collision_params()
-        p.d, p.h, p.r, p.theta_t, p.lambda_max, p.epsilon, p.L = d, h, r, theta_t, lambda_max, epsilon, L
-        nd = plan.ndim
-        g = np.asarray(Gd, float).reshape(nd, nd).ravel(order='F')
-        for i in range(nd * nd):
-            p.Gd[i] = g[i]
-        p.nD = int(nD)
+        p = _coll_params(plan.ndim, d=d, h=h, r=r, theta_t=theta_t, lambda_max=lambda_max, epsilon=epsilon,
+                         L=L, Gd=Gd, nD=nD)
         hnd, n = ctypes.c_void_p(), ctypes.c_int()
         _check(_lib.hp_collision_create(plan.handle, ctypes.byref(p), ctypes.byref(hnd), ctypes.byref(n)))
         self._h, self.plan, self.numR, self.nD = hnd, plan, n.value, int(nD)
+        self.from_tables = False
+
+    @classmethod
+    def from_tables(cls, plan: Plan, lambda_, indR, fcL, fcL_indx):
+        """The operator from given tables ([ix][k], [k], [ix][k][d], [ix][k][d]
+        as returned by tables()), e.g. tables saved by an earlier run."""
+        lam = np.ascontiguousarray(lambda_, np.float64)
+        ind = np.ascontiguousarray(indR, np.int32).ravel()
+        fc = np.ascontiguousarray(fcL, np.float64)
+        ix = np.ascontiguousarray(fcL_indx, np.int16)
+        numR, nD = ind.size, fc.shape[-1]
+        self = cls.__new__(cls)
+        hnd = ctypes.c_void_p()
+        _check(_lib.hp_collision_create_from_tables(plan.handle, numR, nD, ind.ctypes.data, lam.ctypes.data,
+                                                    fc.ctypes.data, ix.ctypes.data, HP_HOST, ctypes.byref(hnd)))
+        self._h, self.plan, self.numR, self.nD = hnd, plan, numR, nD
+        self.from_tables = True
+        return self
 
     def __del__(self):
         h = getattr(self, '_h', None)
@@ -627,7 +667,9 @@ class Collision:
         lam = np.zeros((nx, k)); ind = np.zeros(k, np.int32); om = np.zeros((nx, k, self.plan.ndim))
         fcL = np.zeros((nx, k, nD)); idx = np.zeros((nx, k, nD), np.int16)
         PC = np.zeros((8 * self.plan.B ** 3, 3))
-        ptrs = [ctypes.c_void_p(a.ctypes.data) for a in (lam, ind, om, fcL, idx, PC)]
+        if self.from_tables:
+            om = PC = None
+        ptrs = [ctypes.c_void_p(a.ctypes.data if a is not None else None) for a in (lam, ind, om, fcL, idx, PC)]
         _check(_lib.hp_collision_tables(self._h, *ptrs, HP_HOST))
         return dict(lambda_=lam, indR=ind, omega=om, fcL=fcL, fcL_indx=idx, PC=PC)
 
@@ -640,6 +682,99 @@ class Collision:
         po, _ = _ptr(out, np.float64)
         _check(_lib.hp_collision_df(self._h, ctypes.c_void_p(pf), ctypes.c_void_p(po), mf))
         return out
+
+
+def _coll_params(ndim, d=0.0, h=0.0, r=0.0, theta_t=0.0, lambda_max=0.0, epsilon=0.0, L=0.0, Gd=None, nD=1):
+    p = hp_collision_params()
+    p.d, p.h, p.r, p.theta_t, p.lambda_max, p.epsilon, p.L = d, h, r, theta_t, lambda_max, epsilon, L
+    if Gd is not None:
+        g = np.asarray(Gd, float).reshape(ndim, ndim).ravel(order='F')
+        for i in range(ndim * ndim):
+            p.Gd[i] = g[i]
+    p.nD = int(nD)
+    return p
+
+
+def _x_grid_of(x):
+    """(ndim, Bx, L) of an omega grid x(n, 2Bx, 2Bx[, 2Bx]) (MATLAB layout)."""
+    x = np.asarray(x)
+    nd, N = x.shape[0], x.shape[1]
+    L = -2.0 * float(x.reshape(nd, -1, order='F')[0, 0])
+    ref = _grid(N // 2, L, nd)
+    if x.shape != ref.shape or not np.allclose(x, ref, rtol=0, atol=1e-9 * max(L, 1.0)):
+        raise HPError(HP_ERR_UNSUPPORTED, 'x must be the uniform grid -L/2 + L*(0:2Bx-1)/(2Bx)')
+    return nd, N // 2, L
+
+
+def getLambda_mex(R, x, d, h, r, theta_t, lambda_max, compact=False):
+    """[lambda, indR, PC] = getLambda_mex(R, x, d, h, r, theta_t, lambda_max, false)
+    (propagation/discrete/mex/sources/pendulum_reduced_collision/src/mexLambda.cpp):
+    lambda (numR, 2Bx, 2Bx), indR int32 (numR,) 0-based, PC (3, 2B, 2B, 2B).
+    R must be the Euler-angle grid (the library builds it on the device)."""
+    if compact:
+        raise HPError(HP_ERR_UNSUPPORTED, 'the compact form of the noise-free model is not provided')
+    B = np.asarray(R).shape[2] // 2
+    nd, Bx, L = _x_grid_of(x)
+    plan = get_plan(B, Bx, nd)
+    p = _coll_params(nd, d=d, h=h, r=r, theta_t=theta_t, lambda_max=lambda_max, L=L)
+    n = ctypes.c_int()
+    _check(_lib.hp_collision_lambda(plan.handle, ctypes.byref(p), ctypes.byref(n), None, None, None, HP_HOST))
+    nx = (2 * Bx) ** nd
+    lam = np.zeros((nx, n.value)); ind = np.zeros(n.value, np.int32); PC = np.zeros((8 * B ** 3, 3))
+    _check(_lib.hp_collision_lambda(plan.handle, ctypes.byref(p), ctypes.byref(n), lam.ctypes.data, ind.ctypes.data,
+                                    PC.ctypes.data, HP_HOST))
+    return (lam.T.reshape((n.value,) + (2 * Bx,) * nd, order='F'), ind,
+            PC.T.reshape((3,) + (2 * B,) * 3, order='F'))
+
+
+def getOmega_mex(R, x, indR, epsilon, PC, direction='new'):
+    """Omega_new = getOmega_mex(R, x, indR, epsilon, PC, 'new') (mexOmega.cpp):
+    Omega+ as (ndim, numR, 2Bx, 2Bx)."""
+    if str(direction).lower() != 'new':
+        raise HPError(HP_ERR_UNSUPPORTED, "only the 'new' direction (the hybrid model's reset map) is provided")
+    B = np.asarray(R).shape[2] // 2
+    nd, Bx, L = _x_grid_of(x)
+    plan = get_plan(B, Bx, nd)
+    ind = np.ascontiguousarray(indR, np.int32).ravel()
+    p = _coll_params(nd, epsilon=epsilon, L=L)
+    om = np.zeros(((2 * Bx) ** nd, ind.size, nd))
+    _check(_lib.hp_collision_omega(plan.handle, ctypes.byref(p), ind.size, ind.ctypes.data, om.ctypes.data, HP_HOST))
+    return np.transpose(om, (2, 1, 0)).reshape((nd, ind.size) + (2 * Bx,) * nd, order='F')
+
+
+def getFcL_mex(x, Omega, lambda_, Gd, nD):
+    """[fcL, fcL_indx] = getFcL_mex(x, Omega_new, lambda, Gd, nD) (mexFcL.cpp):
+    (nD, numR, 2Bx, 2Bx) float64 and int16."""
+    nd, Bx, L = _x_grid_of(x)
+    plan = get_plan(2, Bx, nd)
+    Om = np.asarray(Omega, float)
+    numR = Om.shape[1]
+    om = np.ascontiguousarray(np.transpose(Om.reshape(nd, numR, -1, order='F'), (2, 1, 0)))
+    lam = np.ascontiguousarray(np.asarray(lambda_, float).reshape(numR, -1, order='F').T)
+    p = _coll_params(nd, L=L, Gd=Gd, nD=int(nD))
+    nx = (2 * Bx) ** nd
+    fcL = np.zeros((nx, numR, int(nD))); idx = np.zeros((nx, numR, int(nD)), np.int16)
+    _check(_lib.hp_collision_fcL(plan.handle, ctypes.byref(p), numR, om.ctypes.data, lam.ctypes.data,
+                                 fcL.ctypes.data, idx.ctypes.data, HP_HOST))
+    shp = (int(nD), numR) + (2 * Bx,) * nd
+    return (np.transpose(fcL, (2, 1, 0)).reshape(shp, order='F'), np.transpose(idx, (2, 1, 0)).reshape(shp, order='F'))
+
+
+def pendulum_reduced_discrete_propagate(noise, f, lambda_, indR, fcL, fcL_indx):
+    """df = pendulum_reduced_discrete_propagate(true, f, lambda, indR, fcL, fcL_indx)
+    (mexPropagate.cpp:6-77, propagate.cu:6-121) with MATLAB-layout tables."""
+    if not noise:
+        raise HPError(HP_ERR_UNSUPPORTED, 'only the noisy form of the hybrid model is provided')
+    f = np.asfortranarray(f, np.float64)
+    B, Bx, nd = f.shape[0] // 2, f.shape[3] // 2, f.ndim - 3
+    plan = get_plan(B, Bx, nd)
+    lam = np.asarray(lambda_, float)
+    numR = lam.shape[0]
+    nD = np.asarray(fcL).shape[0]
+    c = Collision.from_tables(plan, lam.reshape(numR, -1, order='F').T,
+                              indR, np.transpose(np.asarray(fcL, float).reshape(nD, numR, -1, order='F'), (2, 1, 0)),
+                              np.transpose(np.asarray(fcL_indx, np.int16).reshape(nD, numR, -1, order='F'), (2, 1, 0)))
+    return c.df(f)
 
 
 class Batch:

@@ -30,7 +30,8 @@ enum hp_status {
   HP_ERR_CUDA = 4,        /* a CUDA call failed                          */
   HP_ERR_UNSUPPORTED = 5, /* input outside the supported model class     */
   HP_ERR_NONFINITE = 6,   /* a NaN/Inf guard fired                       */
-  HP_ERR_NO_MODEL = 7     /* propagation requested before hp_plan_set_model */
+  HP_ERR_NO_MODEL = 7,    /* propagation requested before hp_plan_set_model */
+  HP_ERR_MASS_DRIFT = 8   /* the l = 0 mass guard of hp_state_set_guard fired */
 };
 
 enum hp_precision {
@@ -108,10 +109,14 @@ int hp_plan_launch_count(hp_plan* plan, long long* count);
  * HP_BETA_AUTO: the tensor cores (tcgen05, three TF32 products per FP32
  * product) in HP_MIXED plans with B >= 15, CUDA-core FMAs otherwise (FP64
  * plans always); HP_BETA_SIMT: CUDA-core FMAs; HP_BETA_TENSOR: the tensor cores
- * in every HP_MIXED plan.  hp_plan_tc_errors returns how
- * many tensor-core launches of the plan had a wait give up (their outputs are
- * not valid; 0 in normal operation; reading it synchronises the device). */
-enum hp_beta_engine { HP_BETA_AUTO = 0, HP_BETA_SIMT = 1, HP_BETA_TENSOR = 2 };
+ * in every HP_MIXED plan; HP_BETA_TENSOR_BF16: the tensor cores with BF16x3
+ * operands (each operand split into three BF16 parts, six BF16 products per
+ * FP32 product, FP32 accumulation) in every HP_MIXED plan.  hp_plan_tc_errors returns the number of
+ * tensor-core thread blocks of the plan whose bounded wait on the tensor core
+ * gave up since the previous call (their outputs are not valid; the transform
+ * itself still returns HP_OK, so poll this where it matters; 0 in normal
+ * operation); the call synchronises the device and resets the count. */
+enum hp_beta_engine { HP_BETA_AUTO = 0, HP_BETA_SIMT = 1, HP_BETA_TENSOR = 2, HP_BETA_TENSOR_BF16 = 3 };
 int hp_plan_set_beta_engine(hp_plan* plan, int engine);
 int hp_plan_tc_errors(hp_plan* plan, int* count);
 
@@ -211,8 +216,14 @@ int hp_pendulum_adjoint(hp_plan* plan, const double* F0, const double* lamT, int
  *   F, dF   device pointers, full MATLAB layout (as for hp_pendulum_derivative).
  * All scratch lives in one static device array of HP_NOALLOC_SCRATCH_BYTES
  * that every GPU loading the library keeps until the process exits; problems
- * needing more (FP64: 64 bytes, mixed: 48 bytes per stored coefficient row and
- * omega point, plus the tile list) return HP_ERR_SHAPE.  The plan and its model
+ * needing more return HP_ERR_SHAPE.  Per stored coefficient row and omega point
+ * it takes 64 bytes (FP64) or 48 bytes (mixed) on a 3-D omega grid, 48 / 40
+ * bytes on a 2-D grid, plus the plane tile list: about 0.5 M (FP64) / 0.7 M
+ * (mixed) such points in 3-D, 0.7 M / 0.8 M in 2-D.  It covers omega grids of
+ * up to 32 points per axis (2Bx in 4..32; larger grids return
+ * HP_ERR_UNSUPPORTED whatever their size) and the coefficient-gravity models
+ * of hp_plan_set_model (a density-gravity model returns HP_ERR_UNSUPPORTED).
+ * The plan and its model
  * must exist already (hp_plan_create / hp_plan_set_model allocate).  The first
  * call on a device looks up the array's device address, so make that first call
  * before any stream capture.  Every call shares the one array: calls that may
@@ -282,6 +293,35 @@ int hp_collision_destroy(hp_collision* coll);
 int hp_collision_tables(hp_collision* coll, double* lambda, int* indR, double* omega, double* fcL,
                         short* fcL_indx, double* PC, int mem);
 int hp_collision_df(hp_collision* coll, const double* f, double* df, int mem);
+/* The table builders one MEX call at a time, for callers that build, keep or
+ * reload the tables separately as pendulum_reduced_hybrid.m:130-141 does (it
+ * caches fcL in a .mat file).  Tables use the layouts of hp_collision_tables;
+ * all of lambda/indR/omega/fcL/fcL_indx/PC live in `mem`.
+ *   hp_collision_lambda  replaces [lambda,indR,PC] = getLambda_mex(R,x,d,h,r,theta_t,lambda_max,false)
+ *     (.../src/getLambda.cu:8-85, mexLambda.cpp:78-94): uses d, h, r, theta_t,
+ *     lambda_max, L of params; *numR receives the number of colliding
+ *     attitudes; lambda ([ix][k], nx * numR), indR and PC ([iR][3]) may each be
+ *     NULL (call once with NULL to size them).
+ *   hp_collision_omega   replaces Omega_new = getOmega_mex(R,x,indR,epsilon,PC,'new')
+ *     (.../src/getOmega.cu:8-59, 73-92): Omega+ [ix][k][ndim] of the numR
+ *     attitudes indR (ascending, 0-based; others are rejected); uses epsilon, L.
+ *   hp_collision_fcL     replaces [fcL,fcL_indx] = getFcL_mex(x,Omega_new,lambda,Gd,nD)
+ *     (.../src/getFcL.cu:11-166): the nD largest Gaussian taps per landing
+ *     point, normalised per source point, times lambda dx^n; uses Gd, nD, L.
+ *   hp_collision_create_from_tables builds the operator of hp_collision_df and
+ *     hp_state_hybrid_step from given tables, the inputs of
+ *     pendulum_reduced_discrete_propagate(true,f,lambda,indR,fcL,fcL_indx)
+ *     (.../src/mexPropagate.cpp:6-77); the tables are copied, fcL_indx entries
+ *     outside [0, nx) or indR not ascending in [0, (2B)^3) give HP_ERR_INVALID.
+ *     hp_collision_tables then returns lambda, indR, fcL and fcL_indx only. */
+int hp_collision_lambda(hp_plan* plan, const hp_collision_params* params, int* numR, double* lambda, int* indR,
+                        double* PC, int mem);
+int hp_collision_omega(hp_plan* plan, const hp_collision_params* params, int numR, const int* indR, double* omega,
+                       int mem);
+int hp_collision_fcL(hp_plan* plan, const hp_collision_params* params, int numR, const double* omega,
+                     const double* lambda, double* fcL, short* fcL_indx, int mem);
+int hp_collision_create_from_tables(hp_plan* plan, int numR, int nD, const int* indR, const double* lambda,
+                                    const double* fcL, const short* fcL_indx, int mem, hp_collision** coll);
 
 /* ---- initial densities ----
  * Matrix Fisher x Gaussian on the plan's grid, the initial condition of
@@ -363,6 +403,28 @@ int hp_state_density(hp_state* state, void* f);
  * density in the plan's compute precision (fftSO3R_mex('forward',f,d,w),
  * propagation/mex/sources/fftSO3R/kernel.cu:11-195, without host staging). */
 int hp_state_load_density(hp_state* state, const void* f);
+/* Per-step health check of a resident state (no counterpart in the reference,
+ * whose MEX error handlers print and continue, e.g.
+ * propagation/mex/sources/pendulum_propagate_reduced_den/setup.cu:7-37).  Every
+ * check_every steps of hp_state_step / hp_state_hybrid_step the FP64
+ * coefficients are scanned for NaN/Inf (HP_ERR_NONFINITE), and with
+ * mass_rtol > 0 the l = 0 mass F^0_00[0] is compared with its value when the
+ * guard was set (|m - m0| > mass_rtol |m0|: HP_ERR_MASS_DRIFT).  A failed
+ * check ends the call after the failing step, which stays in the state;
+ * hp_last_error names the step.  check_every = 0 turns the guard off.  Each
+ * check synchronises the plan's stream; inside a stream capture the checks
+ * are skipped, and hp_batch_step checks its guarded members after its graph
+ * replays.  The first call allocates a 4-byte device flag. */
+int hp_state_set_guard(hp_state* state, int check_every, double mass_rtol);
+/* Device memory budget of the library (no counterpart in the reference, whose
+ * MEX files allocate and free on every call).  hp_set_device_budget caps the
+ * device bytes the library holds at once over all devices and objects (plan
+ * tables and workspaces, states, collision tables; 0 = no cap); an allocation
+ * beyond the cap fails as a failed cudaMalloc does, with HP_ERR_ALLOC.
+ * hp_device_bytes returns the bytes held now.  The static scratch array of
+ * hp_pendulum_derivative_noalloc is not counted. */
+int hp_set_device_budget(long long bytes);
+int hp_device_bytes(long long* bytes);
 /* F^0_{00}[k=0] (total mass, notes/6 pendulum/pendulum.tex:108-134) of the state. */
 int hp_state_mass(hp_state* state, double* mass);
 /* hp_moments of the resident state; after hybrid steps these are the moments

@@ -43,6 +43,19 @@ def test_argument_validation_without_gpu(hp):
     assert lib.hp_plan_tc_errors(None, ctypes.byref(cnt)) == hp.HP_ERR_INVALID
 
 
+def test_device_budget_and_guard_arguments(hp):
+    lib = hp._lib
+    assert lib.hp_set_device_budget(-5) == hp.HP_ERR_INVALID
+    assert lib.hp_set_device_budget(1 << 20) == hp.HP_OK
+    assert lib.hp_set_device_budget(0) == hp.HP_OK
+    v = ctypes.c_longlong(-1)
+    assert lib.hp_device_bytes(ctypes.byref(v)) == hp.HP_OK and v.value >= 0
+    assert lib.hp_device_bytes(None) == hp.HP_ERR_INVALID
+    assert lib.hp_state_set_guard(None, 1, 0.0) == hp.HP_ERR_INVALID
+    assert lib.hp_collision_lambda(None, None, None, None, None, None, 1) == hp.HP_ERR_INVALID
+    assert lib.hp_collision_create_from_tables(None, 0, 1, None, None, None, None, 1, None) == hp.HP_ERR_INVALID
+
+
 def test_plan_creation_fails_cleanly_without_device(hp):
     import torch
     if torch.cuda.is_available():
@@ -71,21 +84,38 @@ def test_mex_argument_checks(hp):
         hp._fit_gyro(pd.make_OJO(x, Jfull), 3, P.L)
 
 
-@pytest.mark.parametrize('gateway', ['HP_MEX_PROPAGATE3', 'HP_MEX_PROPAGATE2', 'HP_MEX_FFTSO3R',
-                                     'HP_MEX_GYROBIAS'])
-def test_mex_gateway_compiles(gateway):
-    """The MATLAB gateways (one source, one define each) compile against
-    include/hp.h and the MEX API declarations (MATLAB itself is not installed)."""
+GATEWAYS = [('HP_MEX_PROPAGATE3', 'pendulum_propagate', 11), ('HP_MEX_PROPAGATE2', 'pendulum_propagate_reduced', 10),
+            ('HP_MEX_FFTSO3R', 'fftSO3R_mex', None), ('HP_MEX_GYROBIAS', 'gyrobias_propagate', 6),
+            ('HP_MEX_PROPAGATE_DEN', 'pendulum_propagate_reduced_den', 12),
+            ('HP_MEX_DISCRETE', 'pendulum_reduced_discrete_propagate', 6), ('HP_MEX_GETLAMBDA', 'getLambda_mex', 8),
+            ('HP_MEX_GETOMEGA', 'getOmega_mex', 6), ('HP_MEX_GETFCL', 'getFcL_mex', 5)]
+
+
+@pytest.mark.parametrize('define,name,nrhs', GATEWAYS)
+def test_mex_gateway_builds_and_checks_arguments(define, name, nrhs):
+    """Every MATLAB gateway (one source, one define each) builds against
+    include/hp.h, libhp.so and the host-memory MEX runtime of tests/mex_stub,
+    loads, and reports a wrong argument count through mexErrMsgIdAndTxt before
+    it touches the device."""
     import shutil
-    import subprocess
-    cc = shutil.which('gcc')
-    if cc is None:
+    if shutil.which('gcc') is None:
         pytest.skip('no C compiler')
-    here = os.path.dirname(os.path.abspath(__file__))
-    root = os.path.dirname(here)
-    src = os.path.join(root, 'hybridpendulum-up_b200', 'mex', 'hp_mex.c')
-    for extra in ([], ['-DHP_MEX_MIXED']):
-        r = subprocess.run([cc, '-std=c99', '-Wall', '-Werror', '-fsyntax-only', f'-D{gateway}', *extra,
-                            '-I', os.path.join(here, 'mex_stub'), '-I', os.path.join(root, 'include'), src],
-                           capture_output=True, text=True)
-        assert r.returncode == 0, r.stderr
+    import mexrt
+    gw = mexrt.Gateway(mexrt.build_gateway(define, name))
+    if define == 'HP_MEX_PROPAGATE3':
+        mexrt.Gateway(mexrt.build_gateway(define, name + '32', ['-DHP_MEX_MIXED']))
+    with pytest.raises(mexrt.MexError) as e:
+        gw.call()
+    if nrhs is not None:
+        assert f'expected {nrhs} inputs' in str(e.value)
+
+
+def test_mex_gateways_reject_unsupported_forms():
+    """The noise-free forms of the discrete-only study are refused with a message."""
+    import mexrt
+    om = mexrt.Gateway(mexrt.build_gateway('HP_MEX_GETOMEGA', 'getOmega_mex'))
+    with pytest.raises(mexrt.MexError, match="'new' direction"):
+        om.call(np.zeros((3, 3, 2, 2, 2)), np.zeros((2, 4, 4)), np.zeros(1, np.int32), 0.8, np.zeros((3, 8)), 'old')
+    dp = mexrt.Gateway(mexrt.build_gateway('HP_MEX_DISCRETE', 'pendulum_reduced_discrete_propagate'))
+    with pytest.raises(mexrt.MexError, match='noisy form'):
+        dp.call(False, 0.0, 0.0, 0.0, 0.0, 0.0)
