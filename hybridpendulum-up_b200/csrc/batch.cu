@@ -215,6 +215,9 @@ extern "C" int hp_batch_step(hp_batch* b, double dt, int method, int nsteps) {
   const int rs = use_streams(b, false);
   if (st != HP_OK) return st;
   if (e != cudaSuccess) { hp_set_error(cudaGetErrorString(e)); return HP_ERR_CUDA; }
+  // the replayed steps ran no guard checks: check every guarded member now
+  if (nsteps > 0)
+    for (auto s : b->st) BT_CHECK(hp_state_guard_check(s, true));
   return rs;
 }
 

@@ -1,8 +1,12 @@
 // C ABI (include/hp.h): plans, host/device staging, integrators, state API.
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <complex>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 #include "common.cuh"
 #include "plan.hpp"
@@ -11,6 +15,58 @@ using namespace hp;
 
 static thread_local std::string g_err;
 void hp_set_error(const char* msg) { g_err = msg ? msg : ""; }
+
+// ------------------------------------------------ device memory budget ----
+namespace {
+std::mutex g_alloc_mu;
+std::unordered_map<void*, size_t> g_alloc_sizes;
+long long g_alloc_bytes = 0;    // bytes held by the library now
+long long g_alloc_budget = 0;   // 0: no cap
+}  // namespace
+
+cudaError_t hp_dev_alloc_raw(void** p, size_t bytes) {
+  *p = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    if (g_alloc_budget > 0 && g_alloc_bytes + (long long)bytes > g_alloc_budget) return cudaErrorMemoryAllocation;
+  }
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  g_alloc_sizes[*p] = bytes;
+  g_alloc_bytes += (long long)bytes;
+  return cudaSuccess;
+}
+
+cudaError_t hp_dev_free(void* p) {
+  if (!p) return cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    auto it = g_alloc_sizes.find(p);
+    if (it != g_alloc_sizes.end()) {
+      g_alloc_bytes -= (long long)it->second;
+      g_alloc_sizes.erase(it);
+    }
+  }
+  return cudaFree(p);
+}
+
+extern "C" int hp_set_device_budget(long long bytes) {
+  if (bytes < 0) { hp_set_error("budget must be >= 0 (0: no cap)"); return HP_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  g_alloc_budget = bytes;
+  return HP_OK;
+}
+
+extern "C" int hp_device_bytes(long long* bytes) {
+  if (!bytes) { hp_set_error("null argument"); return HP_ERR_INVALID; }
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  *bytes = g_alloc_bytes;
+  return HP_OK;
+}
 extern "C" const char* hp_last_error(void) { return g_err.c_str(); }
 
 #define HP_CHECK(expr)              \
@@ -22,7 +78,7 @@ extern "C" const char* hp_last_error(void) { return g_err.c_str(); }
 void hp_plan::ws_release(const char* name) {
   for (auto& kv : ws)
     if (kv.first == name && kv.second.p) {
-      cudaFree(kv.second.p);
+      hp_dev_free(kv.second.p);
       kv.second = Buf{};
     }
 }
@@ -31,10 +87,10 @@ void* hp_plan::ws_get(const char* name, size_t bytes, int* status) {
   for (auto& kv : ws) {
     if (kv.first == name) {
       if (kv.second.bytes >= bytes) return kv.second.p;
-      cudaFree(kv.second.p);
+      hp_dev_free(kv.second.p);
       kv.second = Buf{};
       void* q = nullptr;
-      if (cudaMalloc(&q, bytes) != cudaSuccess) {
+      if (hp_dev_alloc(&q, bytes) != cudaSuccess) {
         cudaGetLastError();
         hp_set_error("device allocation failed");
         *status = HP_ERR_ALLOC;
@@ -45,7 +101,7 @@ void* hp_plan::ws_get(const char* name, size_t bytes, int* status) {
     }
   }
   void* q = nullptr;
-  if (cudaMalloc(&q, bytes) != cudaSuccess) {
+  if (hp_dev_alloc(&q, bytes) != cudaSuccess) {
     cudaGetLastError();
     hp_set_error("device allocation failed");
     *status = HP_ERR_ALLOC;
@@ -122,8 +178,8 @@ extern "C" int hp_plan_launch_count(hp_plan* p, long long* count) {
 
 extern "C" int hp_plan_set_beta_engine(hp_plan* p, int engine) {
   if (!p) { hp_set_error("null plan"); return HP_ERR_INVALID; }
-  if (engine != HP_BETA_AUTO && engine != HP_BETA_SIMT && engine != HP_BETA_TENSOR) {
-    hp_set_error("engine must be HP_BETA_AUTO, HP_BETA_SIMT or HP_BETA_TENSOR");
+  if (engine != HP_BETA_AUTO && engine != HP_BETA_SIMT && engine != HP_BETA_TENSOR && engine != HP_BETA_TENSOR_BF16) {
+    hp_set_error("engine must be HP_BETA_AUTO, HP_BETA_SIMT, HP_BETA_TENSOR or HP_BETA_TENSOR_BF16");
     return HP_ERR_INVALID;
   }
   p->beta_engine = engine;
@@ -179,11 +235,11 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
 
 extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
-  cudaFree(p->rows); cudaFree(p->seg); cudaFree(p->wig64); cudaFree(p->wig32); cudaFree(p->wfull);
-  cudaFree(p->qw); cudaFree(p->cg1); cudaFree(p->tap_wr); cudaFree(p->tap_wr32);
+  hp_dev_free(p->rows); hp_dev_free(p->seg); hp_dev_free(p->wig64); hp_dev_free(p->wig32); hp_dev_free(p->wfull);
+  hp_dev_free(p->qw); hp_dev_free(p->cg1); hp_dev_free(p->tap_wr); hp_dev_free(p->tap_wr32);
   p->prof_on = false;
   prof_collect(p);
-  for (auto& kv : p->ws) cudaFree(kv.second.p);
+  for (auto& kv : p->ws) hp_dev_free(kv.second.p);
   delete p;
   return HP_OK;
 }
@@ -620,7 +676,7 @@ extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
   // F3 and acc are allocated on first use by a method that needs them
   double2** bufs[2] = {&s->F, &s->F2};
   for (auto b : bufs) {
-    if (cudaMalloc(b, ib) != cudaSuccess) {
+    if (hp_dev_alloc(b, ib) != cudaSuccess) {
       cudaGetLastError();
       hp_state_destroy(s);
       hp_set_error("device allocation failed");
@@ -634,8 +690,9 @@ extern "C" int hp_state_create(hp_plan* p, hp_state** out) {
 
 extern "C" int hp_state_destroy(hp_state* s) {
   if (!s) return HP_OK;
-  cudaFree(s->F); cudaFree(s->F2); cudaFree(s->F3); cudaFree(s->acc); cudaFree(s->fg);
-  cudaFree(s->F32[0]); cudaFree(s->F32[1]);
+  hp_dev_free(s->guard_flag);
+  hp_dev_free(s->F); hp_dev_free(s->F2); hp_dev_free(s->F3); hp_dev_free(s->acc); hp_dev_free(s->fg);
+  hp_dev_free(s->F32[0]); hp_dev_free(s->F32[1]);
   delete s;
   return HP_OK;
 }
@@ -672,10 +729,10 @@ extern "C" int hp_state_store(hp_state* s, double* F, int mem) {
 static int state_bufs(hp_state* s, int method) {
   const size_t ib = 16 * (size_t)s->plan->nrows * s->plan->nx;
   if (method != HP_EULER && !s->F3) {
-    if (cudaMalloc(&s->F3, ib) != cudaSuccess) { cudaGetLastError(); s->F3 = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
+    if (hp_dev_alloc(&s->F3, ib) != cudaSuccess) { cudaGetLastError(); s->F3 = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
   }
   if ((method == HP_RK2 || method == HP_RK4) && !s->acc) {
-    if (cudaMalloc(&s->acc, ib) != cudaSuccess) { cudaGetLastError(); s->acc = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
+    if (hp_dev_alloc(&s->acc, ib) != cudaSuccess) { cudaGetLastError(); s->acc = nullptr; hp_set_error("device allocation failed"); return HP_ERR_ALLOC; }
   }
   return HP_OK;
 }
@@ -692,9 +749,9 @@ extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
   const bool carry = p->ndim == 3 && p->precision == HP_MIXED;
   if (carry && !s->F32[0]) {
     const size_t b32 = 8 * (size_t)p->nrows * p->nx;
-    if (cudaMalloc(&s->F32[0], b32) != cudaSuccess || cudaMalloc(&s->F32[1], b32) != cudaSuccess) {
+    if (hp_dev_alloc(&s->F32[0], b32) != cudaSuccess || hp_dev_alloc(&s->F32[1], b32) != cudaSuccess) {
       cudaGetLastError();
-      cudaFree(s->F32[0]); cudaFree(s->F32[1]);
+      hp_dev_free(s->F32[0]); hp_dev_free(s->F32[1]);
       s->F32[0] = s->F32[1] = nullptr;
       hp_set_error("device allocation failed");
       return HP_ERR_ALLOC;
@@ -711,6 +768,78 @@ extern "C" int hp_state_step(hp_state* s, double dt, int method, int nsteps) {
       s->f32_valid = true;
     } else {
       HP_CHECK(integrate_internal(p, &s->F, &s->F2, &s->F3, s->acc, dt, method));
+    }
+    HP_CHECK(hp_state_guard_check(s, false));
+  }
+  return HP_OK;
+}
+
+// ------------------------------------------------------ health guard ----
+__global__ void k_nonfinite(const double2* __restrict__ a, long long n, int* __restrict__ flag) {
+  bool bad = false;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double2 v = a[i];
+    bad |= !isfinite(v.x) || !isfinite(v.y);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+extern "C" int hp_state_set_guard(hp_state* s, int check_every, double mass_rtol) {
+  if (!s || check_every < 0 || !std::isfinite(mass_rtol)) { hp_set_error("bad argument"); return HP_ERR_INVALID; }
+  if (check_every > 0 && !s->guard_flag) {
+    if (hp_dev_alloc(&s->guard_flag, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      s->guard_flag = nullptr;
+      hp_set_error("device allocation failed");
+      return HP_ERR_ALLOC;
+    }
+  }
+  double m0 = 0.0;
+  if (check_every > 0 && mass_rtol > 0) {
+    HP_CHECK(hp_state_mass(s, &m0));
+    if (!std::isfinite(m0) || m0 == 0.0) { hp_set_error("the state's l = 0 mass is zero or not finite"); return HP_ERR_NONFINITE; }
+  }
+  s->guard_every = check_every;
+  s->guard_rtol = mass_rtol > 0 ? mass_rtol : 0.0;
+  s->guard_mass0 = m0;
+  s->guard_count = 0;
+  return HP_OK;
+}
+
+int hp_state_guard_check(hp_state* s, bool force) {
+  if (s->guard_every <= 0 || !s->guard_flag) return HP_OK;
+  if (!force && ++s->guard_count % s->guard_every) return HP_OK;
+  hp_plan* p = s->plan;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  HP_CUDA_TRY(cudaStreamIsCapturing(p->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return HP_OK;
+  const long long n = p->nrows * p->nx;
+  HP_CUDA_TRY(cudaMemsetAsync(s->guard_flag, 0, sizeof(int), p->stream));
+  {
+    ProfScope _ps(p, "guard", p->stream);
+    const long long nb = std::min<long long>((n + 255) / 256, 148LL * 8);
+    k_nonfinite<<<(unsigned)nb, 256, 0, p->stream>>>(s->F, n, s->guard_flag);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  int flag = 0;
+  const long long row = p->h_seg[(size_t)(0 - p->m_lo) * p->D + p->lmax];
+  double2 m;
+  HP_CUDA_TRY(cudaMemcpyAsync(&flag, s->guard_flag, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaMemcpyAsync(&m, s->F + row * p->nx, sizeof(double2), cudaMemcpyDeviceToHost, p->stream));
+  HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  char msg[160];
+  if (flag) {
+    snprintf(msg, sizeof msg, "non-finite coefficients after step %lld since the guard was set", s->guard_count);
+    hp_set_error(msg);
+    return HP_ERR_NONFINITE;
+  }
+  if (s->guard_rtol > 0) {
+    const double drift = std::fabs(m.x - s->guard_mass0) / std::fabs(s->guard_mass0);
+    if (!(drift <= s->guard_rtol)) {
+      snprintf(msg, sizeof msg, "l = 0 mass drifted by %.3e (tolerance %.3e) after step %lld since the guard was set",
+               drift, s->guard_rtol, s->guard_count);
+      hp_set_error(msg);
+      return HP_ERR_MASS_DRIFT;
     }
   }
   return HP_OK;
@@ -742,7 +871,7 @@ extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int
   HP_CHECK(state_bufs(s, method));
   if (!s->fg) {
     const size_t eb = p->precision == HP_FP64 ? sizeof(double) : sizeof(float);
-    if (cudaMalloc(&s->fg, eb * (size_t)p->n_grid()) != cudaSuccess) {
+    if (hp_dev_alloc(&s->fg, eb * (size_t)p->n_grid()) != cudaSuccess) {
       cudaGetLastError();
       s->fg = nullptr;
       hp_set_error("device allocation failed");
@@ -758,6 +887,7 @@ extern "C" int hp_state_hybrid_step(hp_state* s, hp_collision* c, double dt, int
     HP_CHECK(hp_collision_apply(c, s->fg, dt, st));
     HP_CHECK(hp_forward_internal(p, s->fg, 0, s->F, st));
     s->fg_valid = true;
+    HP_CHECK(hp_state_guard_check(s, false));
   }
   return HP_OK;
 }

@@ -7,10 +7,23 @@
 #define HP_CUDA_TRY(expr)                                                     \
   do {                                                                        \
     cudaError_t _e = (expr);                                                  \
-    if (_e != cudaSuccess) { hp_set_error(cudaGetErrorString(_e)); return HP_ERR_CUDA; } \
+    if (_e != cudaSuccess) {                                                  \
+      hp_set_error(cudaGetErrorString(_e));                                   \
+      return _e == cudaErrorMemoryAllocation ? HP_ERR_ALLOC : HP_ERR_CUDA;    \
+    }                                                                         \
   } while (0)
 
 void hp_set_error(const char* msg);
+
+// Every device allocation of the library goes through these two, so that the
+// process-wide budget of hp_set_device_budget applies to all of them: beyond
+// the budget hp_dev_alloc fails with cudaErrorMemoryAllocation, as cudaMalloc
+// does when the device is full.
+cudaError_t hp_dev_alloc_raw(void** p, size_t bytes);
+cudaError_t hp_dev_free(void* p);
+template <typename T> inline cudaError_t hp_dev_alloc(T** p, size_t bytes) {
+  return hp_dev_alloc_raw(reinterpret_cast<void**>(p), bytes);
+}
 
 namespace hp {
 

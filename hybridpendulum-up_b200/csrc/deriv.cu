@@ -21,6 +21,7 @@
 //   k_plane   : 2-D (k1, k2) work of every remaining term on one k3 plane of a
 //               tile of n-consecutive rows, then out = F0 + a dF (+ acc += b dF).
 // For ndim = 2 the plane pass covers the whole omega grid and k_axis3 is skipped.
+#include <atomic>
 #include <vector>
 #include "common.cuh"
 #include "plan.hpp"
@@ -854,34 +855,42 @@ int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double
 static constexpr size_t kNoAllocScratchBytes = (size_t)HP_NOALLOC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Address of the scratch array on each device, looked up once per device.
-static void* g_noalloc_addr[64] = {nullptr};
+// Address of the scratch array on each device (one context per device, the
+// runtime's primary context), looked up once per device.  Threads that race on
+// the first call store the same value; the atomics make that well defined.
+static std::atomic<void*> g_noalloc_addr[64];
 
 static int noalloc_scratch(void** out) {
   int dev = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) { hp_set_error("device index out of range"); return HP_ERR_INVALID; }
-  if (!g_noalloc_addr[dev]) {
-    void* ptr = nullptr;
+  void* ptr = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!ptr) {
     const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr) {
       hp_set_error(e != cudaSuccess ? cudaGetErrorString(e) : "scratch symbol has no device address");
       return HP_ERR_CUDA;
     }
-    g_noalloc_addr[dev] = ptr;
+    g_noalloc_addr[dev].store(ptr, std::memory_order_release);
   }
-  *out = g_noalloc_addr[dev];
+  *out = ptr;
   return HP_OK;
 }
 
 // Writes the plane-pass tile list (every (m, l) row cut into chunks of CT
-// consecutive n) on the device, so no host buffer is needed.
+// consecutive n) on the device, so no host buffer is needed: one thread per
+// (m, l) row, its first tile at the count of the tiles of the rows before it.
 __global__ void k_make_tiles(int m_lo, int lmax, int CT, PlaneTile* tiles) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  int k = 0;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = 0, r = 0;
   for (int m = m_lo; m <= lmax; ++m)
-    for (int l = abs(m); l <= lmax; ++l)
-      for (int n0 = -l; n0 <= l; n0 += CT) tiles[k++] = PlaneTile{m, l, n0, min(CT, l - n0 + 1)};
+    for (int l = abs(m); l <= lmax; ++l, ++r) {
+      if (r == t) {
+        for (int n0 = -l; n0 <= l; n0 += CT) tiles[k++] = PlaneTile{m, l, n0, min(CT, l - n0 + 1)};
+        return;
+      }
+      k += (2 * l + 1 + CT - 1) / CT;
+    }
 }
 
 static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
@@ -893,9 +902,9 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   constexpr int CT = PlaneCfg<T>::C;
   cudaStream_t s = p->stream;
   const size_t pts = (size_t)p->nrows * p->nx;
-  int ntiles = 0;
+  int ntiles = 0, nml = 0;
   for (int m = p->m_lo; m <= p->lmax; ++m)
-    for (int l = std::abs(m); l <= p->lmax; ++l) ntiles += (2 * l + 1 + CT - 1) / CT;
+    for (int l = std::abs(m); l <= p->lmax; ++l, ++nml) ntiles += (2 * l + 1 + CT - 1) / CT;
   const bool p3 = p->ndim == 3;
   size_t off = 0;
   double2* Fi = reinterpret_cast<double2*>(base + off); off = align256(off + 16 * pts);
@@ -911,7 +920,7 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
   const RowLayout L = p->layout();
   int st = hp_full_to_internal(p, Ffull, Fi, s);
   if (st) return st;
-  k_make_tiles<<<1, 1, 0, s>>>(p->m_lo, p->lmax, CT, tiles);
+  k_make_tiles<<<(nml + 127) / 128, 128, 0, s>>>(p->m_lo, p->lmax, CT, tiles);
   HP_CUDA_TRY(cudaGetLastError());
   if (p3) {
     const long long nt = p->nrows * (long long)N * N;

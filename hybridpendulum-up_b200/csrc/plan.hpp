@@ -102,7 +102,16 @@ struct hp_state {
   float2* F32[2] = {nullptr, nullptr};
   int f32_cur = 0;
   bool f32_valid = false;
+  // per-step health check (hp_state_set_guard): every guard_every steps
+  int guard_every = 0;
+  double guard_rtol = 0.0;      // l = 0 mass drift tolerance (<= 0: not checked)
+  double guard_mass0 = 0.0;     // F^0_00[0] when the guard was set
+  long long guard_count = 0;    // steps since the guard was set
+  int* guard_flag = nullptr;    // device flag of the non-finite scan
 };
+// The check of hp_state_set_guard after a step (force: whatever the count);
+// returns HP_ERR_NONFINITE / HP_ERR_MASS_DRIFT when it fails.
+int hp_state_guard_check(hp_state* s, bool force);
 
 struct hp_collision;
 // f += dt * df(f), in place, f in the plan's compute precision (device).

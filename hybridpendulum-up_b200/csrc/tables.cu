@@ -242,42 +242,42 @@ int hp_tables_build(hp_plan* p) {
       for (int l = l0; l <= lmax; ++l) p->h_rows.push_back(make_char4((char)l, (char)m, (char)n, 0));
     }
   p->nrows = (long long)p->h_rows.size();
-  HP_CUDA_TRY(cudaMalloc(&p->rows, sizeof(char4) * p->nrows));
-  HP_CUDA_TRY(cudaMalloc(&p->seg, sizeof(int) * p->h_seg.size()));
+  HP_CUDA_TRY(hp_dev_alloc(&p->rows, sizeof(char4) * p->nrows));
+  HP_CUDA_TRY(hp_dev_alloc(&p->seg, sizeof(int) * p->h_seg.size()));
   HP_CUDA_TRY(cudaMemcpy(p->rows, p->h_rows.data(), sizeof(char4) * p->nrows, cudaMemcpyHostToDevice));
   HP_CUDA_TRY(cudaMemcpy(p->seg, p->h_seg.data(), sizeof(int) * p->h_seg.size(), cudaMemcpyHostToDevice));
 
   std::vector<double> fact(2 * lmax + 2, 1.0);
   for (int k = 1; k < (int)fact.size(); ++k) fact[k] = fact[k - 1] * k;
   double* dfact = nullptr;
-  HP_CUDA_TRY(cudaMalloc(&dfact, sizeof(double) * fact.size()));
+  HP_CUDA_TRY(hp_dev_alloc(&dfact, sizeof(double) * fact.size()));
   HP_CUDA_TRY(cudaMemcpy(dfact, fact.data(), sizeof(double) * fact.size(), cudaMemcpyHostToDevice));
 
   const long long nwfull = (long long)D * D * (lmax + 1) * 2 * B;
-  HP_CUDA_TRY(cudaMalloc(&p->wfull, sizeof(double) * nwfull));
+  HP_CUDA_TRY(hp_dev_alloc(&p->wfull, sizeof(double) * nwfull));
   HP_CUDA_TRY(cudaMemset(p->wfull, 0, sizeof(double) * nwfull));
-  HP_CUDA_TRY(cudaMalloc(&p->wig64, sizeof(double) * 2 * B * p->nrows));
-  HP_CUDA_TRY(cudaMalloc(&p->wig32, sizeof(float) * 2 * B * p->nrows));
-  HP_CUDA_TRY(cudaMalloc(&p->qw, sizeof(double) * 2 * B));
+  HP_CUDA_TRY(hp_dev_alloc(&p->wig64, sizeof(double) * 2 * B * p->nrows));
+  HP_CUDA_TRY(hp_dev_alloc(&p->wig32, sizeof(float) * 2 * B * p->nrows));
+  HP_CUDA_TRY(hp_dev_alloc(&p->qw, sizeof(double) * 2 * B));
   const int nth = 2 * B * D * D;
   k_wigner<<<(nth + 127) / 128, 128>>>(B, lmax, dfact, p->wfull, p->layout(), p->wig64, p->wig32);
   HP_CUDA_TRY(cudaGetLastError());
   k_weights<<<1, 2 * B>>>(B, p->qw);
   HP_CUDA_TRY(cudaGetLastError());
   const int ncg = (lmax + 1) * 3 * (2 * lmax + 3) * 3;
-  HP_CUDA_TRY(cudaMalloc(&p->cg1, sizeof(double) * ncg));
+  HP_CUDA_TRY(hp_dev_alloc(&p->cg1, sizeof(double) * ncg));
   const int nt_cg = (lmax + 1) * 3 * (2 * lmax + 3);
   k_cg1<<<(nt_cg + 127) / 128, 128>>>(lmax, p->cg1);
   HP_CUDA_TRY(cudaGetLastError());
   HP_CUDA_TRY(cudaDeviceSynchronize());
-  cudaFree(dfact);
+  hp_dev_free(dfact);
   return HP_OK;
 }
 
 int hp_build_gravity_taps(hp_plan* p) {
   if (p->tap_wr) return HP_OK;
-  HP_CUDA_TRY(cudaMalloc(&p->tap_wr, sizeof(double) * 9 * p->nrows));
-  HP_CUDA_TRY(cudaMalloc(&p->tap_wr32, sizeof(float) * 9 * p->nrows));
+  HP_CUDA_TRY(hp_dev_alloc(&p->tap_wr, sizeof(double) * 9 * p->nrows));
+  HP_CUDA_TRY(hp_dev_alloc(&p->tap_wr32, sizeof(float) * 9 * p->nrows));
   const unsigned g = (unsigned)((p->nrows + 127) / 128);
   k_gravity_taps<double><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr);
   k_gravity_taps<float><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr32);

@@ -21,15 +21,24 @@
 // lo are below 2^-21 relative per product.  W's split is taken from the FP64
 // table (lo = x64 - hi), so W carries ~34 significant bits.
 //
+// Precision, second form: BF16x3 (kind::f16 with BF16 operands, FP32
+// accumulation).  Each operand is split three ways, x = b0 + b1 + b2 with
+// b0 = bf16(x), b1 = bf16(x - b0), b2 = bf16(x - b0 - b1) (each remainder is
+// exact in FP32), and D accumulates the six products of order <= 2,
+// A0W0 + A0W1 + A1W0 + A0W2 + A2W0 + A1W1; the dropped terms are of order
+// 2^-24 relative.  Products of two BF16 values are exact in FP32.  W's split
+// is again taken from the FP64 table.
+//
 // Shared-memory operands use the K-major, no-swizzle canonical layout: core
-// matrices of 8 rows x 16 bytes (4 TF32 values), the K chunks of one 8-row
-// group 128 bytes apart (leading byte offset) and the 8-row groups KP*32
-// bytes apart (stride byte offset).  One thread issues the MMAs and commits
+// matrices of 8 rows x 16 bytes (4 TF32 or 8 BF16 values), the K chunks of one
+// 8-row group 128 bytes apart (leading byte offset) and the 8-row groups
+// KC*128 bytes apart (stride byte offset), KC = the 16-byte chunks of a row.  One thread issues the MMAs and commits
 // them to an mbarrier; every warp then reads its 32 TMEM lanes
 // (tcgen05.ld 32x32b) and writes the rows straight into the [row][omega]
 // coefficient layout.
 #include <stdint.h>
 #include <algorithm>
+#include <cuda_bf16.h>
 #include "common.cuh"
 #include "plan.hpp"
 
@@ -38,6 +47,17 @@ namespace {
 
 __device__ __forceinline__ float tf32_rn(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// three-way BF16 split of x (bits of b0 | b1 << 16 and of b2), remainders exact in FP32
+__device__ __forceinline__ void bf16x3_split(float x, uint32_t& b0, uint32_t& b1, uint32_t& b2) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h0);
+  const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(h1);
+  const __nv_bfloat16 h2 = __float2bfloat16_rn(r2);
+  b0 = (uint32_t)__bfloat16_as_ushort(h0);
+  b1 = (uint32_t)__bfloat16_as_ushort(h1);
+  b2 = (uint32_t)__bfloat16_as_ushort(h2);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -52,12 +72,23 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 template <int M, int N> __host__ __device__ constexpr uint32_t idesc_tf32() {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+// kind::f16 with BF16 A and B (format 1 in both type fields), F32 accumulator
+template <int M, int N> __host__ __device__ constexpr uint32_t idesc_bf16() {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accum) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+}
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
 }
 __device__ __forceinline__ void umma_commit(uint32_t mbar) {
@@ -106,9 +137,10 @@ constexpr int TC_M = 128;        // real rows per tile (64 complex omega points)
 constexpr int TC_TMEM_COLS = 32; // accumulator columns allocated (N <= 32)
 
 // Grid: (omega-tile runs, pairs).  Q: the stage-1 tiles as floats,
-// [(mi*2B + q)*2B + b][2*nwc]; tab: [row][2][KP] TF32 hi/lo of w_b d (zero for
-// b >= 2B); out: [row][nx] complex as floats.  err: set to 1 when a wait on the
-// tensor cores gives up.
+// [(mi*2B + q)*2B + b][2*nwc]; tab: per row, the split parts of w_b d (zero for
+// b >= 2B): TF32 [row][2][KP] floats, BF16 [row][3][KP] bf16 values;
+// out: [row][nx] complex as floats.  err: counts the blocks whose wait on the
+// tensor cores gave up.
 // STAGED: the raw tile [b][128 rows] of Q arrives in shared memory by 16-byte
 // cp.async copies issued while the previous tile's MMAs and epilogue run (the
 // whole tile in flight at once, no registers held); the split pass then reads
@@ -117,25 +149,28 @@ constexpr int TC_TMEM_COLS = 32; // accumulator columns allocated (N <= 32)
 // multiples of 32 points); for an odd chunk length the kernel instead loads
 // each row's values into registers, 32 at a time (the GPU tests run only the
 // staged form, since no plan produces an odd chunk).
-template <int KP, int NP, bool STAGED>
-__global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, const float* __restrict__ tab,
+// BF16: the BF16x3 form (KP a multiple of 16); else the 3xTF32 form (KP a
+// multiple of 8).
+template <int KP, int NP, bool STAGED, bool BF16>
+__global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, const void* __restrict__ tabv,
                                                  const int2* __restrict__ pairs, int NB2, long long nwc,
                                                  int tiles_per_cta, float* __restrict__ out, long long nx,
                                                  long long w0, int* __restrict__ err) {
-  static_assert(KP % 8 == 0 && KP <= 64, "K: multiple of 8, at most 64");
+  constexpr int ES = BF16 ? 2 : 4;                 // operand element bytes
+  constexpr int NPL = BF16 ? 3 : 2;                // split planes per operand
+  static_assert(KP % (BF16 ? 16 : 8) == 0 && KP <= 64, "K: multiple of one MMA's K, at most 64");
   static_assert(NP == 16 || NP == 32, "N: 16 or 32");
-  constexpr int KC = KP / 4;                       // 16-byte K chunks per row
+  constexpr int KC = KP * ES / 16;                 // 16-byte K chunks per row
+  constexpr int EC = 16 / ES;                      // elements per chunk
   constexpr uint32_t LBO = 128, SBO = KC * 128;    // bytes
-  constexpr uint32_t A_BYTES = TC_M * KP * 4, B_BYTES = NP * KP * 4;
+  constexpr uint32_t A_BYTES = TC_M * KP * ES, B_BYTES = NP * KP * ES;
   constexpr uint32_t S_BYTES = STAGED ? TC_M * KP * 4 : 0;
-  constexpr uint32_t IDESC = idesc_tf32<TC_M, NP>();
+  constexpr uint32_t IDESC = BF16 ? idesc_bf16<TC_M, NP>() : idesc_tf32<TC_M, NP>();
   extern __shared__ __align__(1024) unsigned char tc_sm[];
-  unsigned char* sAh = tc_sm;
-  unsigned char* sAl = tc_sm + A_BYTES;
-  unsigned char* sBh = tc_sm + 2 * A_BYTES;
-  unsigned char* sBl = tc_sm + 2 * A_BYTES + B_BYTES;
-  float* sS = reinterpret_cast<float*>(tc_sm + 2 * A_BYTES + 2 * B_BYTES);   // raw tile [KP][128]
-  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(tc_sm + 2 * A_BYTES + 2 * B_BYTES + S_BYTES);
+  unsigned char* sA = tc_sm;                                   // NPL planes of A_BYTES
+  unsigned char* sB = tc_sm + NPL * A_BYTES;                   // NPL planes of B_BYTES
+  float* sS = reinterpret_cast<float*>(tc_sm + NPL * (A_BYTES + B_BYTES));   // raw tile [KP][128]
+  uint64_t* mbar_p = reinterpret_cast<uint64_t*>(tc_sm + NPL * (A_BYTES + B_BYTES) + S_BYTES);
   uint32_t* tmem_p = reinterpret_cast<uint32_t*>(mbar_p + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int2 pe = pairs[blockIdx.y];
@@ -168,27 +203,54 @@ __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, co
     for (int e = tid; e < (KP - NB2) * TC_M; e += 128) sS[NB2 * TC_M + e] = 0.f;   // K padding rows
     if (t_begin < t_end) stage(t_begin);
   }
-  // W tile (hi, lo): item (j, K chunk), rows j >= len zero
+  // W tile planes: item (j, K chunk), rows j >= len zero
   for (int it = tid; it < NP * KC; it += 128) {
     const int j = it / KC, kc = it % KC;
-    float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-    if (j < len) {
-      const float* rowp = tab + (size_t)(s + j) * 2 * KP + kc * 4;
-      h = *reinterpret_cast<const float4*>(rowp);
-      l = *reinterpret_cast<const float4*>(rowp + KP);
-    }
     const uint32_t off = (j >> 3) * SBO + kc * 128 + (j & 7) * 16;
-    *reinterpret_cast<float4*>(sBh + off) = h;
-    *reinterpret_cast<float4*>(sBl + off) = l;
+#pragma unroll
+    for (int pl = 0; pl < NPL; ++pl) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (j < len)
+        v = *reinterpret_cast<const uint4*>(static_cast<const unsigned char*>(tabv) +
+                                            ((size_t)(s + j) * NPL + pl) * KP * ES + kc * 16);
+      *reinterpret_cast<uint4*>(sB + pl * B_BYTES + off) = v;
+    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_p;
 
+  // split of this thread's row (r = tid) into the A planes: K chunk kc from x[EC]
+  const uint32_t aoff = (tid >> 3) * SBO + (tid & 7) * 16;   // this thread's row r = tid
+  auto put_chunk = [&](int kc, const float (&x)[EC]) {
+    if constexpr (BF16) {
+      uint32_t w[3][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        uint32_t a0, a1, a2, c0, c1, c2;
+        bf16x3_split(x[2 * u], a0, a1, a2);
+        bf16x3_split(x[2 * u + 1], c0, c1, c2);
+        w[0][u] = a0 | (c0 << 16);
+        w[1][u] = a1 | (c1 << 16);
+        w[2][u] = a2 | (c2 << 16);
+      }
+#pragma unroll
+      for (int pl = 0; pl < 3; ++pl)
+        *reinterpret_cast<uint4*>(sA + pl * A_BYTES + aoff + kc * 128) = make_uint4(w[pl][0], w[pl][1], w[pl][2], w[pl][3]);
+    } else {
+      float4 h, l;
+      h.x = tf32_rn(x[0]); l.x = x[0] - h.x;
+      h.y = tf32_rn(x[1]); l.y = x[1] - h.y;
+      h.z = tf32_rn(x[2]); l.z = x[2] - h.z;
+      h.w = tf32_rn(x[3]); l.w = x[3] - h.w;
+      *reinterpret_cast<float4*>(sA + aoff + kc * 128) = h;
+      *reinterpret_cast<float4*>(sA + A_BYTES + aoff + kc * 128) = l;
+    }
+  };
+
   uint32_t phase = 0;
   bool ok = true;
-  const uint32_t aoff = (tid >> 3) * SBO + (tid & 7) * 16;   // this thread's row r = tid
   for (long long t = t_begin; t < t_end && ok; ++t) {
     const long long r0 = t * TC_M;                          // first real row of the tile
     const long long rows = 2 * nwc - r0 < TC_M ? 2 * nwc - r0 : TC_M;
@@ -198,41 +260,27 @@ __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, co
       __syncthreads();                                      // tile t is in sS
 #pragma unroll
       for (int kc = 0; kc < KC; ++kc) {
-        float x[4];
+        float x[EC];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) x[u] = sS[(kc * 4 + u) * TC_M + tid];
-        float4 h, l;
-        h.x = tf32_rn(x[0]); l.x = x[0] - h.x;
-        h.y = tf32_rn(x[1]); l.y = x[1] - h.y;
-        h.z = tf32_rn(x[2]); l.z = x[2] - h.z;
-        h.w = tf32_rn(x[3]); l.w = x[3] - h.w;
-        *reinterpret_cast<float4*>(sAh + aoff + kc * 128) = h;
-        *reinterpret_cast<float4*>(sAl + aoff + kc * 128) = l;
+        for (int u = 0; u < EC; ++u) x[u] = sS[(kc * EC + u) * TC_M + tid];
+        put_chunk(kc, x);
       }
     } else {
-      // A tile: row r = tid, all K chunks; 8 chunks (32 loads) in flight at a time
+      // A tile: row r = tid, all K chunks; 32 loads in flight at a time
+      constexpr int CB = 32 / EC;                           // chunks per batch
 #pragma unroll
-      for (int k0 = 0; k0 < KC; k0 += 8) {
-        float v[8][4];
+      for (int k0 = 0; k0 < KC; k0 += CB) {
+        float v[CB][EC];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
+        for (int c = 0; c < CB; ++c)
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int b = (k0 + c) * 4 + u;
+          for (int u = 0; u < EC; ++u) {
+            const int b = (k0 + c) * EC + u;
             v[c][u] = (k0 + c < KC && rv && b < NB2) ? __ldg(Qp + (size_t)b * 2 * nwc + r0 + tid) : 0.f;
           }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          if (k0 + c < KC) {
-            float4 h, l;
-            h.x = tf32_rn(v[c][0]); l.x = v[c][0] - h.x;
-            h.y = tf32_rn(v[c][1]); l.y = v[c][1] - h.y;
-            h.z = tf32_rn(v[c][2]); l.z = v[c][2] - h.z;
-            h.w = tf32_rn(v[c][3]); l.w = v[c][3] - h.w;
-            *reinterpret_cast<float4*>(sAh + aoff + (k0 + c) * 128) = h;
-            *reinterpret_cast<float4*>(sAl + aoff + (k0 + c) * 128) = l;
-          }
-        }
+        for (int c = 0; c < CB; ++c)
+          if (k0 + c < KC) put_chunk(k0 + c, v[c]);
       }
     }
     fence_async_smem();   // generic-proxy smem writes -> visible to the tensor core
@@ -240,13 +288,24 @@ __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, co
     __syncthreads();
     tc_fence_after();
     if (tid == 0) {
-      const uint32_t ah = smem_u32(sAh), al = smem_u32(sAl), bh = smem_u32(sBh), bl = smem_u32(sBl);
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
 #pragma unroll
-      for (int kk = 0; kk < KP / 8; ++kk) {
+      for (int kk = 0; kk < KC / 2; ++kk) {                 // one MMA consumes two K chunks
         const uint32_t o = kk * 2 * 128;
-        umma_tf32(tmem, umma_desc(ah + o, LBO, SBO), umma_desc(bh + o, LBO, SBO), IDESC, kk > 0 ? 1u : 0u);
-        umma_tf32(tmem, umma_desc(ah + o, LBO, SBO), umma_desc(bl + o, LBO, SBO), IDESC, 1u);
-        umma_tf32(tmem, umma_desc(al + o, LBO, SBO), umma_desc(bh + o, LBO, SBO), IDESC, 1u);
+        auto ad = [&](int pl) { return umma_desc(a0 + pl * A_BYTES + o, LBO, SBO); };
+        auto bd = [&](int pl) { return umma_desc(b0 + pl * B_BYTES + o, LBO, SBO); };
+        if constexpr (BF16) {
+          umma_bf16(tmem, ad(0), bd(0), IDESC, kk > 0 ? 1u : 0u);
+          umma_bf16(tmem, ad(0), bd(1), IDESC, 1u);
+          umma_bf16(tmem, ad(1), bd(0), IDESC, 1u);
+          umma_bf16(tmem, ad(0), bd(2), IDESC, 1u);
+          umma_bf16(tmem, ad(2), bd(0), IDESC, 1u);
+          umma_bf16(tmem, ad(1), bd(1), IDESC, 1u);
+        } else {
+          umma_tf32(tmem, ad(0), bd(0), IDESC, kk > 0 ? 1u : 0u);
+          umma_tf32(tmem, ad(0), bd(1), IDESC, 1u);
+          umma_tf32(tmem, ad(1), bd(0), IDESC, 1u);
+        }
       }
       umma_commit(mbar);
     }
@@ -257,7 +316,7 @@ __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, co
     ok = __syncthreads_and(mbar_wait(mbar, phase)) != 0;
     phase ^= 1u;
     if (!ok) {
-      if (lane == 0) atomicExch(err, 1);
+      if (tid == 0) atomicAdd(err, 1);   // one count per block whose wait gave up
       break;
     }
     tc_fence_after();
@@ -289,6 +348,24 @@ __global__ void __launch_bounds__(128) k_tc_beta(const float* __restrict__ Q, co
                  : "memory");
 }
 
+// [row][3][KP]: BF16 parts b0, b1, b2 of w_b d^l_mn(beta_b), split from FP64
+__global__ void k_dwtc_table_bf16(RowLayout L, const double* __restrict__ wig, const double* __restrict__ qw, int KP,
+                                  __nv_bfloat16* __restrict__ tab) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * KP) return;
+  const long long r = t / KP;
+  const int b = (int)(t % KP);
+  const int NB2 = 2 * L.B;
+  const double x = b < NB2 ? qw[b] * wig[(size_t)b * L.nrows + r] : 0.0;
+  const __nv_bfloat16 h0 = __double2bfloat16(x);
+  const double r1 = x - (double)__bfloat162float(h0);
+  const __nv_bfloat16 h1 = __double2bfloat16(r1);
+  const double r2 = r1 - (double)__bfloat162float(h1);
+  tab[(r * 3) * KP + b] = h0;
+  tab[(r * 3 + 1) * KP + b] = h1;
+  tab[(r * 3 + 2) * KP + b] = __double2bfloat16(r2);
+}
+
 // [row][2][KP]: TF32 hi and lo parts of w_b d^l_mn(beta_b), from FP64
 __global__ void k_dwtc_table(RowLayout L, const double* __restrict__ wig, const double* __restrict__ qw, int KP,
                              float* __restrict__ tab) {
@@ -303,12 +380,13 @@ __global__ void k_dwtc_table(RowLayout L, const double* __restrict__ wig, const 
   tab[(r * 2 + 1) * KP + b] = (float)(x - (double)hi);
 }
 
-template <int KP, int NP>
-int tc_launch(hp_plan* p, const float2* Qg, const float* tab, const int2* pairs, int npairs, float2* out,
+template <int KP, int NP, bool BF16>
+int tc_launch(hp_plan* p, const float2* Qg, const void* tab, const int2* pairs, int npairs, float2* out,
               long long w0, long long nwc, int* err, cudaStream_t s) {
   const bool staged = nwc % 2 == 0;
-  const size_t smem = 2 * (size_t)TC_M * KP * 4 + 2 * (size_t)NP * KP * 4 + (staged ? (size_t)TC_M * KP * 4 : 0) + 16;
-  auto kern = staged ? k_tc_beta<KP, NP, true> : k_tc_beta<KP, NP, false>;
+  constexpr size_t ES = BF16 ? 2 : 4, NPL = BF16 ? 3 : 2;
+  const size_t smem = NPL * ((size_t)TC_M * KP * ES + (size_t)NP * KP * ES) + (staged ? (size_t)TC_M * KP * 4 : 0) + 16;
+  auto kern = staged ? k_tc_beta<KP, NP, true, BF16> : k_tc_beta<KP, NP, false, BF16>;
   HP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long ntiles = (nwc + TC_M / 2 - 1) / (TC_M / 2);
   // about 16 waves of CTAs over 148 SMs, at least 2 tiles per CTA
@@ -331,31 +409,52 @@ int tc_beta_forward(hp_plan* p, const float2* Qg, const int2* pairs, int npairs,
     hp_set_error("tensor-core beta contraction: FP32 plans with B <= 32 only");
     return HP_ERR_UNSUPPORTED;
   }
-  const int KP = (2 * p->B + 7) / 8 * 8;
+  const bool bf16 = p->beta_engine == HP_BETA_TENSOR_BF16;
+  const int KP = bf16 ? (2 * p->B + 15) / 16 * 16 : (2 * p->B + 7) / 8 * 8;
   int st = HP_OK;
-  bool have = false;
-  for (auto& kv : p->ws) if (kv.first == "tf.dwtc") have = true;
-  float* tab = (float*)p->ws_get("tf.dwtc", sizeof(float) * 2 * (size_t)p->nrows * KP, &st);
+  const char* tkey = bf16 ? "tf.dwtc16" : "tf.dwtc";
+  bool have = false, have_err = false;
+  for (auto& kv : p->ws) {
+    if (kv.first == tkey) have = true;
+    if (kv.first == "tf.tcerr") have_err = true;
+  }
+  void* tab = p->ws_get(tkey, (bf16 ? 3 * sizeof(__nv_bfloat16) : 2 * sizeof(float)) * (size_t)p->nrows * KP, &st);
   if (st) return st;
   int* err = (int*)p->ws_get("tf.tcerr", sizeof(int), &st);
   if (st) return st;
+  if (!have_err) HP_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
   if (!have) {
-    HP_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
     const long long n = p->nrows * KP;
-    k_dwtc_table<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), p->wig64, p->qw, KP, tab);
+    if (bf16)
+      k_dwtc_table_bf16<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), p->wig64, p->qw, KP,
+                                                                     (__nv_bfloat16*)tab);
+    else
+      k_dwtc_table<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->layout(), p->wig64, p->qw, KP, (float*)tab);
     HP_CUDA_TRY(cudaGetLastError());
   }
-  ProfScope _ps(p, "tf.anal.beta.tc", s);
+  ProfScope _ps(p, bf16 ? "tf.anal.beta.tc16" : "tf.anal.beta.tc", s);
   const bool n16 = p->B <= 16;
+  if (bf16) {
+    switch (KP) {
+      case 16: return n16 ? tc_launch<16, 16, true>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s)
+                          : tc_launch<16, 32, true>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+      case 32: return tc_launch<32, 16, true>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+      case 48: return tc_launch<48, 32, true>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+      case 64: return tc_launch<64, 32, true>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+      default:
+        hp_set_error("tensor-core beta contraction: unsupported node count");
+        return HP_ERR_UNSUPPORTED;
+    }
+  }
   switch (KP) {
-    case 8: return n16 ? tc_launch<8, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s)
-                       : tc_launch<8, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 16: return tc_launch<16, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 24: return tc_launch<24, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 32: return tc_launch<32, 16>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 40: return tc_launch<40, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 48: return tc_launch<48, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
-    case 64: return tc_launch<64, 32>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 8: return n16 ? tc_launch<8, 16, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s)
+                       : tc_launch<8, 32, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 16: return tc_launch<16, 16, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 24: return tc_launch<24, 16, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 32: return tc_launch<32, 16, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 40: return tc_launch<40, 32, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 48: return tc_launch<48, 32, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
+    case 64: return tc_launch<64, 32, false>(p, Qg, tab, pairs, npairs, out, w0, nwc, err, s);
     default:
       hp_set_error("tensor-core beta contraction: unsupported node count");
       return HP_ERR_UNSUPPORTED;
@@ -367,6 +466,7 @@ int tc_beta_errors(hp_plan* p, int* count) {
   for (auto& kv : p->ws)
     if (kv.first == "tf.tcerr") {
       HP_CUDA_TRY(cudaMemcpy(count, kv.second.p, sizeof(int), cudaMemcpyDeviceToHost));
+      HP_CUDA_TRY(cudaMemset(kv.second.p, 0, sizeof(int)));   // counted from the last read on
     }
   return HP_OK;
 }

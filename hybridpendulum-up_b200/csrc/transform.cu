@@ -891,7 +891,8 @@ static int anal2_launch(hp_plan* p, const void* f, const double* mult, c2<T>* ou
     if constexpr (sizeof(T) == 4) {
       // AUTO: tensor cores from B = 15 (B=15, 32x32: 0.046 vs 0.052 ms; B=30: 0.24 vs
       // 0.50 ms), CUDA cores below (B=8: 0.015 vs 0.009 ms, set-up dominates)
-      const bool tc = p->beta_engine == HP_BETA_TENSOR || (p->beta_engine == HP_BETA_AUTO && p->B >= 15);
+      const bool tc = p->beta_engine == HP_BETA_TENSOR || p->beta_engine == HP_BETA_TENSOR_BF16 ||
+                      (p->beta_engine == HP_BETA_AUTO && p->B >= 15);
       if (tc && tc_beta_supported(p)) {
         st = tc_beta_forward(p, reinterpret_cast<const float2*>(Qg), dpairs, NPAIR, reinterpret_cast<float2*>(out),
                              w0, nw, s);

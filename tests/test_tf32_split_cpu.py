@@ -11,6 +11,11 @@ numpy for the pairs of B = 15 and B = 30 (w_b d from the oracle) and checks it
 against the FP64 contraction of the same FP32 inputs: within the 1e-6 relative
 L2 bar of the mixed-precision path, while one TF32 product per FP32 product is
 not, which is why the split is there.
+
+The second form, BF16x3 (kind::f16 with BF16 operands), splits each operand
+three ways, x = b0 + b1 + b2 (b_i = bf16 round-to-nearest of the remainder,
+each remainder exact in FP32; W's split from FP64), and sums the six products
+of order <= 2 in FP32; every BF16 x BF16 product is exact in FP32.
 """
 import numpy as np
 import pytest
@@ -62,3 +67,42 @@ def test_three_tf32_products_meet_the_fp32_bar(B):
     assert r3 < 1e-6, r3
     assert r3 < 5 * r32 + 1e-7, (r3, r32)   # on par with plain FP32 arithmetic
     assert r1 > 1e-5, r1                    # a single TF32 product misses the bar
+
+
+def bf16_rn(x):
+    """Round FP32 to BF16 (nearest, ties to even) and back to FP32."""
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return r.view(np.float32)
+
+
+def bf16x3(x64_or_32):
+    x = np.asarray(x64_or_32, np.float64)
+    b0 = bf16_rn(x.astype(np.float32))
+    r1 = x - b0.astype(np.float64)
+    b1 = bf16_rn(r1.astype(np.float32))
+    r2 = r1 - b1.astype(np.float64)
+    b2 = bf16_rn(r2.astype(np.float32))
+    return b0, b1, b2
+
+
+@pytest.mark.parametrize('B', [15, 30, 32])
+def test_bf16x3_products_meet_the_fp32_bar(B):
+    rng = np.random.default_rng(100 + B)
+    nw = 128
+    err = err1 = ref = 0.0
+    for W64 in pair_tables(B, ms=(0, 1, B // 2, B - 1)):
+        Q32 = rng.standard_normal((2 * B, nw)).astype(np.float32)
+        D64 = W64 @ Q32.astype(np.float64)
+        a0, a1, a2 = bf16x3(Q32)
+        w0, w1, w2 = bf16x3(W64)
+        f32 = np.float32
+        D = (w0 @ a0).astype(f32) + (w1 @ a0).astype(f32) + (w0 @ a1).astype(f32) \
+            + (w2 @ a0).astype(f32) + (w0 @ a2).astype(f32) + (w1 @ a1).astype(f32)
+        D1 = bf16_rn(W64.astype(np.float32)) @ bf16_rn(Q32)
+        err += float(np.sum((D.astype(np.float64) - D64) ** 2))
+        err1 += float(np.sum((D1 - D64) ** 2))
+        ref += float(np.sum(D64 ** 2))
+    r, r1 = np.sqrt(err / ref), np.sqrt(err1 / ref)
+    assert r < 1e-6, r
+    assert r1 > 1e-4, r1                    # one BF16 product is far from the bar

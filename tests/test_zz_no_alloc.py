@@ -4,7 +4,8 @@ allocate device memory while they run (all scratch in one static device array).
 Collected last on purpose: a failure here leaves every other test already run.
 Compared with the allocating entry point hp_pendulum_derivative on the same
 inputs, through the C ABI, on two calls in a row (the second with different
-inputs, so stale scratch contents would show).
+inputs, so stale scratch contents would show), and with the FP64 oracle's
+derivative.
 """
 import ctypes
 
@@ -56,7 +57,8 @@ def test_noalloc_matches_allocating_derivative(hp, ndim, precision):
     P, plan = _setup(hp, ndim, precision)
     fn = _fn(hp)
     for call, seed in enumerate((1, 2)):
-        F = torch.from_numpy(np.asfortranarray(_coeffs(P, seed)).ravel(order='F')).cuda()
+        Fh = _coeffs(P, seed)
+        F = torch.from_numpy(np.asfortranarray(Fh).ravel(order='F')).cuda()
         ref = plan.derivative(F)
         out = torch.full_like(F, complex(float('nan'), float('nan')))
         rc = fn(plan.handle, F.data_ptr(), out.data_ptr())
@@ -64,6 +66,20 @@ def test_noalloc_matches_allocating_derivative(hp, ndim, precision):
         torch.cuda.synchronize()
         assert torch.isfinite(torch.view_as_real(out)).all(), f'call {call}: output not fully written'
         assert _rel(out, ref) < TOL[precision], f'call {call}'
+        oracle = pd.derivative_fast(Fh, P)
+        got = out.cpu().numpy().reshape(Fh.shape, order='F')
+        assert np.linalg.norm(got - oracle) / np.linalg.norm(oracle) < TOL[precision], f'call {call}'
+
+
+def test_noalloc_rejects_grids_above_32_points(hp):
+    """The plane tiles of the allocation-free path hold at most 32 points per
+    axis; a 40-point grid is refused (the allocating path takes it)."""
+    import torch
+    P = pd.pendulum_reduced(2, 20)
+    plan = hp.Plan(2, 20, 2, hp.HP_FP64, hp.HP_REAL)
+    plan.set_model(P.L, P.b, P.G, P.MR)
+    buf = torch.zeros(16, dtype=torch.complex128, device='cuda')
+    assert _fn(hp)(plan.handle, buf.data_ptr(), buf.data_ptr()) == hp.HP_ERR_UNSUPPORTED
 
 
 def test_noalloc_rejects_oversized_problem(hp):
