@@ -54,8 +54,13 @@ def parse():
                          'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega); '
                          'forward: one FP32 forward transform on a 2-D omega grid (--B, --Bx, --beta-engine)')
     ap.add_argument('--members', type=int, default=64)
-    ap.add_argument('--beta-engine', default='auto', choices=['auto', 'simt', 'tensor'],
-                    help='forward-transform beta contraction (transform and hybrid workloads)')
+    ap.add_argument('--tc-form', type=int, default=-1, choices=[-1, 0, 1],
+                    help='forward workload: tensor-core kernel form (1 warp-specialised TMA pipeline, 0 staged)')
+    ap.add_argument('--no-autotune', action='store_true',
+                    help='keep the hand-picked launch shapes instead of timing the candidates first')
+    ap.add_argument('--beta-engine', default='auto', choices=['auto', 'simt', 'tensor', 'tensor_bf16'],
+                    help='forward-transform beta contraction (transform, hybrid and forward workloads): '
+                         'tensor = 3xTF32, tensor_bf16 = BF16x3 on the tcgen05 tensor cores')
     return ap.parse_args()
 
 
@@ -243,7 +248,7 @@ def cpu_baseline_obj(B, Bx, steps=1):
             'sample': f'FP64 numpy oracle (restatement, fast form: omega FFTs, degree-1 CG gravity), '
                       f'B={B} on a {2 * Bs}^3 omega grid, {steps} step(s) of Euler propagate + density '
                       f'synthesis, {sec:.2f} s/step, scaled by omega points x{scale:.0f} to {2 * Bx}^3 '
-                      f'(omega-FFT log factor ignored, which favours the CPU)'}
+                      f'(cost per omega point taken as constant in the grid size)'}
 
 
 # ------------------------------------------------------------ replicas ----
@@ -308,6 +313,9 @@ def main():
         return pl
 
     pmix, p64 = make(hp.HP_MIXED), make(hp.HP_FP64)
+    tunes = {}
+    if not args.no_autotune:     # launch shapes timed on scratch, before (and outside) the timed region
+        tunes = {'mixed': pmix.autotune(), 'fp64': p64.autotune()}
     f0 = initial_density_dev(torch, inp, B, Bx, L, dev)
     F0 = torch.zeros(int(np.prod(p64.F_shape)), dtype=torch.complex128, device=dev)
     p64.forward(f0, out=F0)
@@ -330,20 +338,23 @@ def main():
             torch.distributed.barrier()
 
     def timed(state, fout, plan, K, W, profile=False):
+        # the clock sampler (200 ms period) starts before the warm-up so that
+        # its samples cover the whole timed region
+        clk = Clocks(local)
+        clk.start()
         for _ in range(W):
             step(state, fout)
         barrier()
         if profile:
             plan.profile(True)
         n0 = plan.launch_count()
-        clk = Clocks(local)
-        clk.start()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(K):
             step(state, fout)
         ev1.record(stream)
         barrier()
+        time.sleep(0.25)                 # one more sample after the timed region
         clocks = clk.stop()
         ms = ev0.elapsed_time(ev1)
         prof = plan.profile_read() if profile else {}
@@ -457,7 +468,8 @@ def main():
                    'B': B, 'omega_grid': f'{2 * Bx}^3', 'ndim': 3, 'dt': dt, 'method': 'euler',
                    'parallelism': f'replicas x{world}', 'l2': 'inputs larger than L2 (F state 1.24 GB)',
                    'step_includes': ['derivative (Lie, damping, gyroscopic, CG gravity, diffusion)',
-                                     'Euler update (FP64)', 'inverse omega FFT', 'SO(3) synthesis to f']},
+                                     'Euler update (FP64)', 'inverse omega FFT', 'SO(3) synthesis to f'],
+                   'launch_shapes': tunes or 'hand-picked (--no-autotune)'},
         'fp64': {'value': round(value64, 3), 'ms_per_step': round(ms_64 / K64, 4), 'steps': K64,
                  'clocks_sm_mhz': clocks64.get('sm_mhz'),
                  'kernel_ms_per_launch': {k: round(v[0] / max(v[1], 1), 4) for k, v in prof64.items()}},
@@ -482,8 +494,7 @@ def bench_batch(args, rank, world, local):
     omega grids {16^3, 24^3, 32^3} mixed by the seed, advanced together in
     mixed precision (one CUDA graph per two batch steps, members on distinct
     plans concurrent), against the per-density FP64 loop.  The step is the
-    plain pendulum propagation (the collision reset map of the reference is
-    defined for 2-D omega only).  Prints one JSON line (not the headline)."""
+    plain pendulum propagation.  Prints one JSON line (not the headline)."""
     import torch
     torch.cuda.set_device(local)
     dev = torch.device('cuda', local)
@@ -544,6 +555,8 @@ def bench_batch(args, rank, world, local):
     # the batch (mixed precision)
     for key in sorted(set(shapes)):
         plans[key] = plan(key[0], key[1], hp.HP_MIXED)
+        if not args.no_autotune:
+            plans[key].autotune()
     states = []
     for k, sh in enumerate(shapes):
         st = hp.State(plans[sh])
@@ -655,9 +668,11 @@ def bench_transform(args, rank, local):
             'config': {'workload': 'transform precision stress', 'B': B, 'omega_grid': '24^3',
                        'coefficients': 'i.i.d. N(0,1)/(2l+1), complex', 'beta_engine': args.beta_engine},
             'fp64': out['fp64'], 'mixed': out['mixed'],
-            'beta_contraction': {'forward': 'tcgen05 tensor cores, 3xTF32 split (mixed; --beta-engine simt: CUDA cores)',
-                                 'backward': 'CUDA cores, fused with the gamma/alpha FFTs'},
-            'not_built': 'BF16x3-split beta contraction'}
+            'beta_contraction': {'forward': {'auto': 'tcgen05 tensor cores, 3xTF32 split (B >= 15)',
+                                             'tensor': 'tcgen05 tensor cores, 3xTF32 split',
+                                             'tensor_bf16': 'tcgen05 tensor cores, BF16x3 split',
+                                             'simt': 'CUDA-core FP32 FMAs'}[args.beta_engine],
+                                 'backward': 'CUDA cores, fused with the gamma/alpha FFTs'}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -674,6 +689,8 @@ def bench_forward(args, rank, local):
     B, Bx = args.B, args.Bx
     plan = hp.Plan(B, Bx, 2, hp.HP_MIXED, hp.HP_REAL)
     plan.set_beta_engine(beta_engine(hp, args))
+    if args.tc_form >= 0:
+        plan.set_tune(tc_form=args.tc_form)
     g = torch.Generator(device='cuda').manual_seed(11 + rank)
     f = torch.rand((2 * B) ** 3 * (2 * Bx) ** 2, dtype=torch.float32, device='cuda', generator=g)
     st = hp.State(plan)
@@ -698,14 +715,15 @@ def bench_forward(args, rank, local):
             'dtype': 'f32', 'data': 'synthetic (uniform random density)',
             'config': {'workload': 'forward transform', 'B': B, 'omega_grid': f'{2 * Bx}x{2 * Bx}',
                        'beta_engine': args.beta_engine},
-            'kernel_ms_per_launch': fam, 'tc_errors': plan.tc_errors()}
+            'kernel_ms_per_launch': fam, 'tc_errors': plan.tc_errors(), 'launch_shapes': plan.get_tune()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
 
 
 def beta_engine(hp, args):
-    return {'auto': hp.HP_BETA_AUTO, 'simt': hp.HP_BETA_SIMT, 'tensor': hp.HP_BETA_TENSOR}[args.beta_engine]
+    return {'auto': hp.HP_BETA_AUTO, 'simt': hp.HP_BETA_SIMT, 'tensor': hp.HP_BETA_TENSOR,
+            'tensor_bf16': hp.HP_BETA_TENSOR_BF16}[args.beta_engine]
 
 
 def bench_hybrid(args, rank, local):

@@ -48,7 +48,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_plan_set_gyro_bias_model', 'hp_gyrobias_propagate', 'hp_fftSO3_real_forward',
            'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod', 'hp_plan_set_beta_engine', 'hp_plan_tc_errors',
            'hp_collision_lambda', 'hp_collision_omega', 'hp_collision_fcL', 'hp_collision_create_from_tables',
-           'hp_state_set_guard', 'hp_set_device_budget', 'hp_device_bytes']
+           'hp_state_set_guard', 'hp_set_device_budget', 'hp_device_bytes', 'hp_plan_autotune',
+           'hp_plan_set_tune', 'hp_plan_get_tune', 'hp_tune_cache_save', 'hp_tune_cache_load']
 
 
 class HPError(RuntimeError):
@@ -159,6 +160,11 @@ def _load():
         'hp_state_set_guard': [vp, ip, dp],
         'hp_set_device_budget': [ctypes.c_longlong],
         'hp_device_bytes': [ctypes.POINTER(ctypes.c_longlong)],
+        'hp_plan_autotune': [vp, ctypes.POINTER(dp), ctypes.POINTER(dp)],
+        'hp_plan_set_tune': [vp, ip, ip, ip, ip],
+        'hp_plan_get_tune': [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)],
+        'hp_tune_cache_save': [ctypes.c_char_p],
+        'hp_tune_cache_load': [ctypes.c_char_p],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -297,6 +303,21 @@ class Plan:
         (tensor cores in HP_MIXED plans with B >= 15), HP_BETA_SIMT or
         HP_BETA_TENSOR (tensor cores in every HP_MIXED plan)."""
         _check(_lib.hp_plan_set_beta_engine(self._h, int(engine)))
+
+    def autotune(self) -> dict:
+        """Time the candidate launch shapes of this plan's transforms and keep
+        the fastest (cached for later plans of the same key)."""
+        b, f = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.hp_plan_autotune(self._h, ctypes.byref(b), ctypes.byref(f)))
+        return dict(self.get_tune(), backward_ms=b.value, forward_ms=f.value)
+
+    def set_tune(self, synth_pt: int = 0, synth_waves: int = 0, tc_waves: int = 0, tc_form: int = -1):
+        _check(_lib.hp_plan_set_tune(self._h, int(synth_pt), int(synth_waves), int(tc_waves), int(tc_form)))
+
+    def get_tune(self) -> dict:
+        a, b, c, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.hp_plan_get_tune(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d)))
+        return dict(synth_pt=a.value, synth_waves=b.value, tc_waves=c.value, tc_form=d.value)
 
     def tc_errors(self) -> int:
         """Tensor-core launches of this plan whose wait gave up (0 normally)."""
@@ -598,6 +619,16 @@ class State:
 def set_device_budget(nbytes: int):
     """Cap the device bytes the library may hold at once (0: no cap)."""
     _check(_lib.hp_set_device_budget(int(nbytes)))
+
+
+def tune_cache_save(path: str):
+    """Write the launch shapes found by Plan.autotune in this process to a text file."""
+    _check(_lib.hp_tune_cache_save(os.fsencode(path)))
+
+
+def tune_cache_load(path: str):
+    """Read a file written by tune_cache_save; later plans of a listed key start from its shapes."""
+    _check(_lib.hp_tune_cache_load(os.fsencode(path)))
 
 
 def device_bytes() -> int:

@@ -183,6 +183,7 @@ extern "C" int hp_plan_set_beta_engine(hp_plan* p, int engine) {
     return HP_ERR_INVALID;
   }
   p->beta_engine = engine;
+  hp_tune_apply_cached(p);   // a tuned shape for this engine, if one was found earlier
   return HP_OK;
 }
 
@@ -229,6 +230,7 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
   for (int a = 0; a < ndim; ++a) p->nx *= p->N;
   int st = hp_tables_build(p);
   if (st) { hp_plan_destroy(p); return st; }
+  hp_tune_apply_cached(p);
   *out = p;
   return HP_OK;
 }

@@ -125,6 +125,24 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
+// ------------------------------------------------------ L2 cache hints ----
+// Streams written once and read only by a later kernel (density, updated
+// coefficients) are stored with an evict-first L2 policy, so that they do not
+// push out lines that blocks running at the same time still read (the
+// synthesis blocks of one omega chunk share their coefficient rows, the plane
+// tiles of one row their halo rows).
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void st_evict_first(double2* a, double2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(a), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_evict_first(float2* a, float2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
+}
+
 // ------------------------------------------------- register-resident FFT ----
 // Small DFT of radix R in registers (out-of-place on v).
 template <int R, bool INV, typename C>

@@ -484,6 +484,7 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
 
   // ---- S6: dF = A + Y1' + G ; out = F0 + a dF ; acc += bacc dF ----
   {
+    const uint64_t pol = l2_policy_evict_first();
     const int tot = tl.cnt * N * N;
     for (int e0 = tid; e0 < tot; e0 += 4 * nth) {
       C g[4];
@@ -511,8 +512,10 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
         double2 o = f0[u];
         o.x += a * dx;
         o.y += a * dy;
-        out[gi[u]] = o;
-        if (out32) out32[gi[u]] = cvt<C, double2>(o);   // the next step's compute-precision input
+        // written once here and read by later kernels: evict first, so the
+        // halo rows other tiles of this plane still read stay in L2
+        st_evict_first(out + gi[u], o, pol);
+        if (out32) st_evict_first(out32 + gi[u], cvt<C, double2>(o), pol);   // the next step's compute-precision input
         if (acc) {
           double2 v = ac[u];
           v.x += bacc * dx;

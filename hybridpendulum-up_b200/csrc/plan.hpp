@@ -67,6 +67,13 @@ struct hp_plan {
 
   // engine of the forward transform's beta contraction (enum hp_beta_engine)
   int beta_engine = 0;
+  // launch shapes chosen by hp_plan_autotune (defaults: the hand-picked ones)
+  struct Tune {
+    int synth_pt = 1;      // omega points per beta-stage item of the synthesis (1, 2, 4; FP32)
+    int synth_waves = 8;   // resident waves of synthesis blocks per SM set
+    int tc_waves = 16;     // waves of tensor-core CTAs of the forward beta contraction
+    int tc_form = 0;       // 0: the staged tensor-core kernel, 1: the warp-specialised TMA-fed one
+  } tune;
 
   // profiling
   bool prof_on = false;
@@ -134,6 +141,9 @@ struct ProfScope {
   ProfScope(hp_plan* plan, const char* name, cudaStream_t stream);
   ~ProfScope();
 };
+
+// launch shapes found earlier by hp_plan_autotune for the plan's key, if any
+void hp_tune_apply_cached(hp_plan* p);
 
 // ---- launchers implemented in the .cu files (return hp_status) ----
 int hp_tables_build(hp_plan* p);

@@ -22,10 +22,23 @@ using namespace hp;
 // ------------------------------------------------------------ omega FFTs ----
 static int smem_limit();
 
+// Omega-blocked layout of the synthesis input: blocks of blk consecutive omega
+// points, each block holding every row's blk values contiguously,
+// [w / blk][row][w % blk].  One synthesis batch (blk = P omega points) then
+// reads a single contiguous run of nrows * P values, and the rows of one
+// (m, n) pair (consecutive in l) sit P values apart.
+__host__ __device__ __forceinline__ long long omega_block_index(long long w, long long row, long long nrows, int blk) {
+  return (w / blk * nrows + row) * blk + w % blk;
+}
+
 // 2-D FFT over (k1, k2) of every (row, k3) plane; one block per (row, k3).
+// blk > 0: the output goes to the omega-blocked layout of the synthesis input
+// (see omega_block_index), plane pl holding omega points pl_w0 .. pl_w0 + N^2 of
+// row pl / planes_per_row.
 template <int N, typename Tin, typename T, bool INV>
 __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, c2<T>* __restrict__ out,
-                                                long long nplanes, T scale) {
+                                                long long nplanes, T scale, int blk = 0, long long nrows = 0,
+                                                int planes_per_row = 1) {
   using C = c2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);   // [N][N+1]
@@ -64,21 +77,36 @@ __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, 
     for (int j = 0; j < N; ++j) sm[j * (N + 1) + k1] = scale * x[j];
   }
   __syncthreads();
+  if (blk > 0) {
+    const long long row = pl / planes_per_row, w0 = (pl % planes_per_row) * (long long)(N * N);
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x)
+      out[omega_block_index(w0 + e, row, nrows, blk)] = sm[(e / N) * (N + 1) + e % N];
+    return;
+  }
   C* dst = out + pl * N * N;
   for (int e = threadIdx.x; e < N * N; e += blockDim.x) dst[e] = sm[(e / N) * (N + 1) + e % N];
 }
 
 // 1-D FFT along the last omega axis (stride N^2) of a [row][N^3] array.
+// blk > 0: in and out are in the omega-blocked layout (N^2 a multiple of blk).
 template <int N, typename T, bool INV>
 __global__ void __launch_bounds__(128) k_wline(const c2<T>* __restrict__ in, c2<T>* __restrict__ out,
-                                               long long nrows, T scale) {
+                                               long long nrows, T scale, int blk = 0) {
   using C = c2<T>;
   constexpr long long plane = (long long)N * N;
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= nrows * plane) return;
   const long long row = t / plane, p = t % plane;
-  const C* src = in + row * plane * N + p;
   C x[N];
+  if (blk > 0) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) x[j] = in[omega_block_index(j * plane + p, row, nrows, blk)];
+    fft<N, INV>(x);
+#pragma unroll
+    for (int j = 0; j < N; ++j) out[omega_block_index(j * plane + p, row, nrows, blk)] = scale * x[j];
+    return;
+  }
+  const C* src = in + row * plane * N + p;
 #pragma unroll
   for (int j = 0; j < N; ++j) x[j] = src[j * plane];
   fft<N, INV>(x);
@@ -117,9 +145,10 @@ __device__ __forceinline__ int synth_swz(int i, int rot) { return (i & ~3) | ((i
 // both addresses 16-byte aligned, size a multiple of 16 bytes.  The issuing
 // thread later waits for the source to have been read (wait_group.read) before
 // the buffer is rewritten, and for completion (wait_group) before exit.
-__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, unsigned bytes) {
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, unsigned bytes, uint64_t pol) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(ssrc);
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(s), "r"(bytes)
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;" ::"l"(gdst), "r"(s),
+               "r"(bytes), "l"(pol)
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
@@ -139,20 +168,23 @@ __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
 
 // Block = (group of NB consecutive beta indices, range of omega points), the
 // (2l+1)-weighted d values of its betas resident in shared memory.  Input rows
-// are read in the [row][omega] layout with the P omega points of a batch on
-// consecutive lanes, so every coefficient load is coalesced; the per-(omega,
-// beta) intermediates G -> H live in shared memory as [bb][m][q][p].
+// are read in the omega-blocked layout [w / P][row][w % P] (omega_block_index):
+// one batch of P omega points is one contiguous run of nrows * P values, the
+// rows of an (m, n) pair P values apart, and the P points of a row on
+// consecutive lanes; the per-(omega, beta) intermediates G -> H live in shared
+// memory as [bb][m][q][p].
 // GD: the (2l+1) d table of the block's betas is read from a global table
 // [group][row][NB] (large bandlimits, where it does not fit shared memory)
 // instead of being staged from the d table `wig`.
-// AF: the coefficients of each batch arrive in a shared-memory tile [row][P]
-// by cp.async issued during the previous batch's FFT and store stages, so the
-// beta contraction reads shared memory (P >= 4: 512 threads, one block per SM;
-// P < 4: 256 threads, two blocks per SM).
-template <int B, typename T, int NB, int P, bool CPLX, bool GD, bool AF = false>
-__global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (sizeof(T) == 8 ? 1 : 2))
+// PT: omega points per beta-stage item (1, 2 or 4, dividing P): an item
+// computes the NB x PT tile of one (m, n) pair, so each coefficient load (PT
+// consecutive omega points, one vector load) feeds NB x PT complex FMAs and
+// each d value PT of them.
+template <int B, typename T, int NB, int P, bool CPLX, bool GD, int PT = 1>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
     k_synth(RowLayout L, const c2<T>* __restrict__ Fp, const T* __restrict__ wig, const int2* __restrict__ pairs,
             void* __restrict__ fout, int nbatch) {
+  static_assert(P % PT == 0, "PT divides P");
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
   constexpr int NM = CPLX ? D : B;
@@ -172,9 +204,7 @@ __global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (
   const int nrows = (int)L.nrows;
   T* sds = reinterpret_cast<T*>(smraw);
   int2* spairs = reinterpret_cast<int2*>(smraw + (GD ? 0 : ((size_t)NB * nrows * sizeof(T) + 15) / 16 * 16));
-  C* scoef = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
-  C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(scoef) +
-                               (AF ? ((size_t)nrows * P * sizeof(C) + 15) / 16 * 16 : 0));
+  C* sG = reinterpret_cast<C*>(reinterpret_cast<unsigned char*>(spairs) + ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16);
   // beta groups of one omega chunk are consecutive blocks, so they read the
   // same coefficient rows close together in time (L2 reuse)
   constexpr int NGROUPS = (NB2 + NB - 1) / NB;
@@ -193,56 +223,69 @@ __global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (
   const long long nx = L.nx;
   // vector and bulk stores need a 16-byte aligned density buffer
   const bool fout_al16 = (reinterpret_cast<unsigned long long>(fout) & 15ull) == 0;
-  // AF: rows of P omega points from w in 16-byte pieces; pieces past nx are
-  // (partly) zero-filled by the copy itself
-  constexpr int CPP = AF ? (int)(P * sizeof(C) / 16) : 1;   // pieces per row
-  auto coef_fetch = [&](long long w) {
-    for (int e = tid; e < nrows * CPP; e += nth) {
-      const int r = e / CPP, pc16 = e % CPP;
-      const long long wp = w + (long long)pc16 * (16 / (long long)sizeof(C));
-      const long long left = (nx - wp) * (long long)sizeof(C);
-      const int nb = left >= 16 ? 16 : (left > 0 ? (int)left : 0);
-      cp_async16_n(scoef + (size_t)r * P + pc16 * (16 / sizeof(C)), Fp + (size_t)r * nx + (nb ? wp : 0), nb);
-    }
-  };
-  if (AF && (long long)chunk * nbatch * P < nx) coef_fetch((long long)chunk * nbatch * P);
   for (int bt = 0; bt < nbatch; ++bt) {
     const long long w0 = ((long long)chunk * nbatch + bt) * P;
     if (w0 >= nx) break;
     if (BULK && fout_al16) bulk_wait_read_all();   // the previous batch's runs have left the staging (aliases sG)
-    if (AF) cp_async_wait_all();                   // this batch's coefficient tile
     __syncthreads();
     // beta stage: item (pair, p), p fastest.  Pairs come from the block's copy
     // of the pair table (longest l-runs first, so the lanes of a warp run
     // loops of similar length); the l-run is loaded in batches of 8 ahead of
     // its FMAs, each coefficient feeding NB FMAs per component.
-    for (int it = tid; it < NPAIR * P; it += nth) {
-      const int p = it % P;
-      const int2 pe = spairs[it / P];
+    constexpr int NPG = P / PT;                 // omega groups of PT points per batch
+    for (int it = tid; it < NPAIR * NPG; it += nth) {
+      const int p0 = (it % NPG) * PT;
+      const int2 pe = spairs[it / NPG];
       const int s = pe.x, len = pe.y & 0xff, mi = (pe.y >> 8) & 0xff, q = (pe.y >> 16) & 0xff;
-      C acc[NB];
+      C acc[NB][PT];
 #pragma unroll
-      for (int bb = 0; bb < NB; ++bb) acc[bb] = czero<C>();
-      if (w0 + p < nx) {
-        const C* src = Fp + (size_t)s * nx + w0 + p;
+      for (int bb = 0; bb < NB; ++bb)
+#pragma unroll
+        for (int pt = 0; pt < PT; ++pt) acc[bb][pt] = czero<C>();
+      if (w0 + p0 < nx) {
+        // the batch's block of the omega-blocked input; rows P values apart
+        const C* src = Fp + ((size_t)(w0 / P) * nrows + s) * P + p0;
         const T* dsrc = sd + (size_t)s * NB;
-        constexpr int JB = 8;
+        // a vector load per row where the PT points are all inside the grid
+        const bool full = w0 + p0 + PT <= nx;
+        constexpr int JB = PT >= 4 ? 4 : 8;
 #pragma unroll
         for (int j0 = 0; j0 < B; j0 += JB) {
           if (j0 < len) {
-            C v[JB];
+            C v[JB][PT];
 #pragma unroll
-            for (int u = 0; u < JB; ++u)
-              v[u] = (j0 + u < len) ? (AF ? scoef[(size_t)(s + j0 + u) * P + p] : src[(size_t)(j0 + u) * nx])
-                                    : czero<C>();
+            for (int u = 0; u < JB; ++u) {
+              const bool ok = j0 + u < len;
+              if constexpr (PT > 1 && sizeof(T) == 4) {
+                if (ok && full) {
+#pragma unroll
+                  for (int h = 0; h < PT / 2; ++h) {
+                    const float4 w4 = *reinterpret_cast<const float4*>(src + (size_t)(j0 + u) * P + 2 * h);
+                    v[u][2 * h] = mk(w4.x, w4.y);
+                    v[u][2 * h + 1] = mk(w4.z, w4.w);
+                  }
+                } else {
+#pragma unroll
+                  for (int pt = 0; pt < PT; ++pt)
+                    v[u][pt] = (ok && w0 + p0 + pt < nx) ? src[(size_t)(j0 + u) * P + pt] : czero<C>();
+                }
+              } else {
+#pragma unroll
+                for (int pt = 0; pt < PT; ++pt)
+                  v[u][pt] = (ok && (PT == 1 || w0 + p0 + pt < nx)) ? src[(size_t)(j0 + u) * P + pt] : czero<C>();
+              }
+            }
 #pragma unroll
             for (int u = 0; u < JB; ++u) {
               if (j0 + u < len) {
 #pragma unroll
                 for (int bb = 0; bb < NB; ++bb) {
                   const T dv = dsrc[(j0 + u) * NB + bb];
-                  acc[bb].x = fma(dv, v[u].x, acc[bb].x);
-                  acc[bb].y = fma(dv, v[u].y, acc[bb].y);
+#pragma unroll
+                  for (int pt = 0; pt < PT; ++pt) {
+                    acc[bb][pt].x = fma(dv, v[u][pt].x, acc[bb][pt].x);
+                    acc[bb][pt].y = fma(dv, v[u][pt].y, acc[bb][pt].y);
+                  }
                 }
               }
             }
@@ -251,14 +294,15 @@ __global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (
       }
 #pragma unroll
       for (int bb = 0; bb < NB; ++bb) {
-        C* g = sG + (bb * NM + mi) * GS + p;
-        g[q * P] = acc[bb];
-        if (pe.y >> 24) g[B * P] = czero<C>();
+#pragma unroll
+        for (int pt = 0; pt < PT; ++pt) {
+          C* g = sG + (bb * NM + mi) * GS + p0 + pt;
+          g[q * P] = acc[bb][pt];
+          if (pe.y >> 24) g[B * P] = czero<C>();
+        }
       }
     }
     __syncthreads();
-    // the next batch's coefficients stream in while this one runs its FFT and store stages
-    if (AF && bt + 1 < nbatch && w0 + P < nx) coef_fetch(w0 + P);
     // gamma stage: item (bb, mi, p): FFT over n -> c, in place
     for (int it = tid; it < NB * NM * P; it += nth) {
       C* g = sG + (it / P) * GS + it % P;
@@ -334,11 +378,12 @@ __global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (
     const int pc = (int)min((long long)P, nx - w0);
     constexpr int RUN = NB * NB2;
     if (BULK && fout_al16) {
+      const uint64_t pol = l2_policy_evict_first();   // the density is written once, read by later kernels
       for (int run = tid; run < pc * NB2; run += nth) {
         const int pp = run / NB2, cc = run % NB2;
         const size_t gi = ((size_t)(w0 + pp) * NB2 + cc) * NB2 * NB2 + (size_t)b0 * NB2;
         bulk_s2g(reinterpret_cast<T*>(fout) + gi, reinterpret_cast<const T*>(sG) + (pp * NB2 + cc) * RS,
-                 (unsigned)(nbv * NB2 * sizeof(T)));
+                 (unsigned)(nbv * NB2 * sizeof(T)), pol);
       }
       bulk_commit();
       continue;
@@ -370,7 +415,6 @@ __global__ void __launch_bounds__(AF && P >= 4 ? 512 : 256, AF && P >= 4 ? 1 : (
     }
   }
   if (BULK && fout_al16) bulk_wait_all();   // shared memory must outlive the bulk copies reading it
-  if (AF) cp_async_wait_all();
 }
 
 // -------------------------------------------------------------- drivers ----
@@ -383,19 +427,21 @@ static int smem_limit() {
 }
 
 template <int N, typename Tin, typename T>
-static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s) {
-  // in/out [row][nx]; in may equal out only when Tin == T
+static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s, int blk = 0) {
+  // in/out [row][nx]; in may equal out only when Tin == T.  blk > 0 (inverse
+  // only): out in the omega-blocked layout of the synthesis input.
   const T scale = inv ? (T)1 / (T)p->nx : (T)1;
-  const long long nplanes = p->nrows * (p->ndim == 3 ? N : 1);
+  const int ppr = p->ndim == 3 ? N : 1;
+  const long long nplanes = p->nrows * ppr;
   const size_t smem = sizeof(c2<T>) * N * (N + 1);
   auto plane = [&](T sc) -> int {
     ProfScope _ps(p, "tf.wplane", s);
     if (inv) {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc);
+      k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
     } else {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc);
+      k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
     }
     HP_CUDA_TRY(cudaGetLastError());
     return HP_OK;
@@ -406,8 +452,8 @@ static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaSt
     if (st) return st;
     const long long nt = p->nrows * (long long)N * N;
     ProfScope _ps(p, "tf.wline", s);
-    if (inv) k_wline<N, T, true><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
-    else k_wline<N, T, false><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale);
+    if (inv) k_wline<N, T, true><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale, blk);
+    else k_wline<N, T, false><<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(out, out, p->nrows, scale, blk);
     HP_CUDA_TRY(cudaGetLastError());
     return HP_OK;
   }
@@ -415,20 +461,20 @@ static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaSt
 }
 
 template <typename Tin, typename T>
-static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s) {
+static int omega_fft_any(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaStream_t s, int blk = 0) {
   switch (p->N) {
-    case 4: return omega_fft<4, Tin, T>(p, in, out, inv, s);
-    case 6: return omega_fft<6, Tin, T>(p, in, out, inv, s);
-    case 8: return omega_fft<8, Tin, T>(p, in, out, inv, s);
-    case 12: return omega_fft<12, Tin, T>(p, in, out, inv, s);
-    case 16: return omega_fft<16, Tin, T>(p, in, out, inv, s);
-    case 20: return omega_fft<20, Tin, T>(p, in, out, inv, s);
-    case 24: return omega_fft<24, Tin, T>(p, in, out, inv, s);
-    case 30: return omega_fft<30, Tin, T>(p, in, out, inv, s);
-    case 32: return omega_fft<32, Tin, T>(p, in, out, inv, s);
-    case 40: return omega_fft<40, Tin, T>(p, in, out, inv, s);
-    case 48: return omega_fft<48, Tin, T>(p, in, out, inv, s);
-    case 60: return omega_fft<60, Tin, T>(p, in, out, inv, s);
+    case 4: return omega_fft<4, Tin, T>(p, in, out, inv, s, blk);
+    case 6: return omega_fft<6, Tin, T>(p, in, out, inv, s, blk);
+    case 8: return omega_fft<8, Tin, T>(p, in, out, inv, s, blk);
+    case 12: return omega_fft<12, Tin, T>(p, in, out, inv, s, blk);
+    case 16: return omega_fft<16, Tin, T>(p, in, out, inv, s, blk);
+    case 20: return omega_fft<20, Tin, T>(p, in, out, inv, s, blk);
+    case 24: return omega_fft<24, Tin, T>(p, in, out, inv, s, blk);
+    case 30: return omega_fft<30, Tin, T>(p, in, out, inv, s, blk);
+    case 32: return omega_fft<32, Tin, T>(p, in, out, inv, s, blk);
+    case 40: return omega_fft<40, Tin, T>(p, in, out, inv, s, blk);
+    case 48: return omega_fft<48, Tin, T>(p, in, out, inv, s, blk);
+    case 60: return omega_fft<60, Tin, T>(p, in, out, inv, s, blk);
     default:
       hp_set_error("omega grid size 2Bx not supported (4, 6, 8, 12, 16, 20, 24, 30, 32, 40, 48, 60)");
       return HP_ERR_UNSUPPORTED;
@@ -473,9 +519,18 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
     return p;
   }
   static constexpr int P = pick_p();
-  // coefficient tile by cp.async (one 512-thread block per SM); off unless chosen below
-  static constexpr bool AF = false;
 };
+
+// Omega block of the synthesis input (P of the synthesis configuration).
+template <typename T, bool CPLX>
+static int synth_block(const hp_plan* p) {
+  switch (p->B) {
+#define X(b) case b: return SynthCfg<b, T, CPLX>::P;
+    X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(24) X(30) X(32)
+#undef X
+    default: return 1;
+  }
+}
 
 // (m, n) pairs with their row start, l-run length, m slot and n bin, longest
 // runs first (the order keeps the lanes of a warp on loops of similar length)
@@ -537,9 +592,7 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
                                         : (size_t)P * NB2 * RS * sizeof(T));
   constexpr int NPAIR = NM * (2 * B - 1);
   const size_t pr_bytes = ((size_t)NPAIR * sizeof(int2) + 15) / 16 * 16;
-  constexpr bool AF = Cfg::AF;
-  const size_t cf_bytes = AF ? ((size_t)p->nrows * P * sizeof(C) + 15) / 16 * 16 : 0;
-  const size_t smem = sd_bytes + pr_bytes + cf_bytes + sg_bytes;
+  const size_t smem = sd_bytes + pr_bytes + sg_bytes;
   if (smem > (size_t)smem_limit()) {
     hp_set_error("synthesis tables exceed shared memory for this bandlimit");
     return HP_ERR_UNSUPPORTED;
@@ -570,17 +623,26 @@ static int synth_launch(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
     dtab = sdg;
   }
   const long long nbatches = (p->nx + P - 1) / P;
-  // about 8 resident waves of blocks over 148 SMs
-  constexpr int NT = AF && P >= 4 ? 512 : 256;
-  long long gx = std::max(1LL, (148LL * (NT == 512 ? 1 : 2) * 8) / ngroups);
+  // synth_waves (8 unless tuned) resident waves of blocks over 148 SMs
+  constexpr int NT = 256;
+  long long gx = std::max(1LL, (148LL * (sizeof(T) == 8 ? 1 : 2) * p->tune.synth_waves) / ngroups);
   int nbatch = (int)std::max(1LL, (nbatches + gx - 1) / gx);
   gx = (nbatches + nbatch - 1) / nbatch;
-  HP_CUDA_TRY(cudaFuncSetAttribute(k_synth<B, T, NB, P, CPLX, GD, AF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)(gx * ngroups), 1);
-  ProfScope _ps(p, "tf.synth", s);
-  k_synth<B, T, NB, P, CPLX, GD, AF><<<grid, NT, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
-  HP_CUDA_TRY(cudaGetLastError());
-  return HP_OK;
+  // omega points per beta-stage item: the plan's tuned choice (FP32 plans; 1 otherwise)
+  const int pt = (sizeof(T) == 4 && P % p->tune.synth_pt == 0) ? p->tune.synth_pt : 1;
+  auto launch = [&](auto kern) -> int {
+    HP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ProfScope _ps(p, "tf.synth", s);
+    kern<<<grid, NT, smem, s>>>(p->layout(), Fp, dtab, dpairs, f, nbatch);
+    HP_CUDA_TRY(cudaGetLastError());
+    return HP_OK;
+  };
+  if constexpr (sizeof(T) == 4) {
+    if (pt == 2 && P % 2 == 0) return launch(k_synth<B, T, NB, P, CPLX, GD, (P % 2 == 0 ? 2 : 1)>);
+    if (pt == 4 && P % 4 == 0) return launch(k_synth<B, T, NB, P, CPLX, GD, (P % 4 == 0 ? 4 : 1)>);
+  }
+  return launch(k_synth<B, T, NB, P, CPLX, GD, 1>);
 }
 
 
@@ -599,17 +661,25 @@ static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
 }
 
 
-template <typename T>
-static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s) {
+// Inverse omega FFT of every row into the omega-blocked synthesis input (a
+// plan workspace sized for whole blocks), then the synthesis.
+template <typename Tin, typename T>
+static int backward_rows(hp_plan* p, const c2<Tin>* Fint, void* f, int complex_out, cudaStream_t s) {
   using C = c2<T>;
   int st = HP_OK;
-  const size_t fb = sizeof(C) * (size_t)p->nrows * p->nx;
+  const int blk = complex_out ? synth_block<T, true>(p) : synth_block<T, false>(p);
+  const size_t fb = sizeof(C) * (size_t)p->nrows * ((p->nx + blk - 1) / blk * blk);
   C* t1 = (C*)p->ws_get("tf.t1", fb, &st);
   if (st) return st;
-  st = omega_fft_any<double, T>(p, Fint, t1, true, s);
+  st = omega_fft_any<Tin, T>(p, Fint, t1, true, s, blk);
   if (st) return st;
   if (complex_out) return synth_any<T, true>(p, t1, f, s);
   return synth_any<T, false>(p, t1, f, s);
+}
+
+template <typename T>
+static int backward_T(hp_plan* p, const double2* Fint, void* f, int complex_out, cudaStream_t s) {
+  return backward_rows<double, T>(p, Fint, f, complex_out, s);
 }
 
 // Forward transform of (mult .) f into [row][omega] coefficients of type c2<T>.
@@ -961,13 +1031,7 @@ int hp_backward_internal(hp_plan* p, const double2* Fint, void* f, int complex_o
 int hp_backward_internal32(hp_plan* p, const float2* Fint32, void* f, int complex_out, cudaStream_t s) {
   if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
   if (p->precision != HP_MIXED) { hp_set_error("FP32 coefficients need a mixed-precision plan"); return HP_ERR_INVALID; }
-  int st = HP_OK;
-  float2* t1 = (float2*)p->ws_get("tf.t1", sizeof(float2) * (size_t)p->nrows * p->nx, &st);
-  if (st) return st;
-  st = omega_fft_any<float, float>(p, Fint32, t1, true, s);
-  if (st) return st;
-  if (complex_out) return synth_any<float, true>(p, t1, f, s);
-  return synth_any<float, false>(p, t1, f, s);
+  return backward_rows<float, float>(p, Fint32, f, complex_out, s);
 }
 
 int hp_forward_internal(hp_plan* p, const void* f, int complex_in, double2* Fint, cudaStream_t s) {

@@ -120,6 +120,29 @@ enum hp_beta_engine { HP_BETA_AUTO = 0, HP_BETA_SIMT = 1, HP_BETA_TENSOR = 2, HP
 int hp_plan_set_beta_engine(hp_plan* plan, int engine);
 int hp_plan_tc_errors(hp_plan* plan, int* count);
 
+/* Launch-shape tuning (no counterpart in the reference).  The knobs are the
+ * runtime launch shapes of the transforms: synth_pt, the omega points per item
+ * of the synthesis beta stage (1, 2 or 4; FP32 plans), synth_waves, the
+ * resident waves of synthesis blocks (how many omega chunks a block walks),
+ * tc_waves, the waves of tensor-core CTAs of the forward beta contraction, and
+ * tc_form, its kernel (1: the warp-specialised pipeline fed by TMA tensor
+ * copies, 0: the staged single-warpgroup kernel).
+ * hp_plan_autotune times every candidate on scratch of the plan's sizes (one
+ * coefficient state and one grid density, allocated and freed by the call)
+ * with CUDA events on the plan's stream, keeps the fastest, and records it in
+ * a process-wide cache keyed by (B, Bx, ndim, precision, symmetry, beta
+ * engine); plans created (or given a beta engine) later with the same key
+ * start from the cached shapes.  backward_ms / forward_ms (may be NULL)
+ * receive the best median transform times (forward: 0 when the forward
+ * transform does not use the tensor cores).  hp_tune_cache_save/load write
+ * and read the cache as a text file, one key and its shapes per line.
+ * hp_plan_set_tune sets knobs by hand (0 keeps a knob, -1 for tc_form). */
+int hp_plan_autotune(hp_plan* plan, double* backward_ms, double* forward_ms);
+int hp_plan_set_tune(hp_plan* plan, int synth_pt, int synth_waves, int tc_waves, int tc_form);
+int hp_plan_get_tune(const hp_plan* plan, int* synth_pt, int* synth_waves, int* tc_waves, int* tc_form);
+int hp_tune_cache_save(const char* path);
+int hp_tune_cache_load(const char* path);
+
 /* Model for the propagation entry points.  MR: complex (2lmax+1,2lmax+1,lmax+1,ndim)
  * in the full layout; only its degree-1, m2=0 block may be non-zero (the
  * gravity term of pendulum.m:166-192 depends on R through R^T e3 only);

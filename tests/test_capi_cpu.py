@@ -56,6 +56,23 @@ def test_device_budget_and_guard_arguments(hp):
     assert lib.hp_collision_create_from_tables(None, 0, 1, None, None, None, None, 1, None) == hp.HP_ERR_INVALID
 
 
+def test_tune_cache_file_round_trip(hp, tmp_path):
+    """The autotuner's cache file format: lines read back and written again
+    unchanged; malformed lines are reported."""
+    src = tmp_path / 'tune.txt'
+    src.write_text('# comment\n15 16 3 1 0 0 2 8 16 1\n30 30 2 1 0 2 4 16 32 0\n')
+    hp.tune_cache_load(str(src))
+    out = tmp_path / 'out.txt'
+    hp.tune_cache_save(str(out))
+    lines = [l for l in out.read_text().splitlines() if not l.startswith('#')]
+    assert '15 16 3 1 0 0 2 8 16 1' in lines and '30 30 2 1 0 2 4 16 32 0' in lines
+    bad = tmp_path / 'bad.txt'
+    bad.write_text('15 16 3 1 0 0 3 8 16 1\n')        # synth_pt 3 is not a choice
+    with pytest.raises(hp.HPError):
+        hp.tune_cache_load(str(bad))
+    assert hp._lib.hp_plan_set_tune(None, 1, 1, 1, 1) == hp.HP_ERR_INVALID
+
+
 def test_plan_creation_fails_cleanly_without_device(hp):
     import torch
     if torch.cuda.is_available():
