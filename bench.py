@@ -54,6 +54,11 @@ def parse():
                          'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega); '
                          'forward: one FP32 forward transform on a 2-D omega grid (--B, --Bx, --beta-engine)')
     ap.add_argument('--members', type=int, default=64)
+    ap.add_argument('--persistent', action='store_true',
+                    help='batch workload: plane passes of the plain members in one persistent launch per round')
+    ap.add_argument('--coll-gb', type=float, default=24.0,
+                    help='batch workload: device memory for 3-D collision tables; the members whose plans fit '
+                         '(smallest first) run the hybrid step with the collision reset map')
     ap.add_argument('--tc-form', type=int, default=-1, choices=[-1, 0, 1],
                     help='forward workload: tensor-core kernel form (1 warp-specialised TMA pipeline, 0 staged)')
     ap.add_argument('--no-autotune', action='store_true',
@@ -493,8 +498,13 @@ def bench_batch(args, rank, world, local):
     """Independent seeded densities with bandlimits B in {8, 12, 16, 20} and
     omega grids {16^3, 24^3, 32^3} mixed by the seed, advanced together in
     mixed precision (one CUDA graph per two batch steps, members on distinct
-    plans concurrent), against the per-density FP64 loop.  The step is the
-    plain pendulum propagation.  Prints one JSON line (not the headline)."""
+    plans concurrent, launch shapes autotuned per plan), against the
+    per-density FP64 loop.  Members whose plans' collision tables fit in
+    --coll-gb (smallest plans first; the 3-D tables hold numR x nx x nD taps)
+    take the hybrid step of pendulum_reduced_hybrid.m:224-234 with the 3-D
+    collision reset map (propagate, backward transform, collision update,
+    forward transform); the others the plain propagation.  Prints one JSON
+    line (not the headline)."""
     import torch
     torch.cuda.set_device(local)
     dev = torch.device('cuda', local)
@@ -525,6 +535,27 @@ def bench_batch(args, rank, world, local):
             Q.append(q)
         return Q[0], np.sort(r.uniform(5, 20, 3))[::-1], Q[1], r.uniform(-1, 1, 3)
 
+    # which plans take the collision reset map: count the colliding attitudes
+    # (cheap), then admit plans smallest-table first within the memory budget
+    CPRM = dict(d=0.12, h=0.2, r=0.025, theta_t=5 * math.pi / 180, lambda_max=100.0, epsilon=0.8)
+    Gd3 = (0.05 * np.eye(3)) @ (0.05 * np.eye(3)).T
+    nD = 10
+    table_bytes = {}
+    for key in sorted(set(shapes)):
+        numR = hp.collision_count(plan(key[0], key[1], hp.HP_FP64), L=L, **{k: CPRM[k] for k in
+                                                                          ('d', 'h', 'r', 'theta_t', 'lambda_max')})
+        nx = (2 * key[1]) ** 3
+        # FP64 tables (lambda, Omega+, fcL, 16-bit indices) + transposed copies in the compute precision
+        table_bytes[key] = numR * nx * (8 + 24 + nD * 10 + (nD * 6 + 4))
+    hybrid_plans, used = set(), 0
+    for key in sorted(table_bytes, key=lambda k: table_bytes[k]):
+        if used + table_bytes[key] <= args.coll_gb * 1e9:
+            hybrid_plans.add(key)
+            used += table_bytes[key]
+
+    def stepper(st, c):
+        return (lambda n: st.hybrid_step(c, dt, 'euler', n)) if c is not None else (lambda n: st.step(dt, 'euler', n))
+
     # per-density FP64 loop (timed on every member, a few steps each)
     k64 = 3
     t64 = 0.0
@@ -532,38 +563,43 @@ def bench_batch(args, rank, world, local):
     nsample = 2
     for key in sorted(set(shapes)):
         p64 = plan(key[0], key[1], hp.HP_FP64)
+        c64 = hp.Collision(p64, L=L, Gd=Gd3, nD=nD, **CPRM) if key in hybrid_plans else None
         st = hp.State(p64)
+        adv = stepper(st, c64)
         for k, sh in enumerate(shapes):
             if sh != key:
                 continue
             U, s_, V, mu = params(k)
             st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
-            st.step(dt, 'euler', 1)
+            adv(1)
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            st.step(dt, 'euler', k64)
+            adv(k64)
             e1.record()
             torch.cuda.synchronize(dev)
             t64 += e0.elapsed_time(e1)
             if k < nsample:
                 st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
-                st.step(dt, 'euler', args.warmup + args.steps)
+                adv(args.warmup + args.steps)
                 ref[k] = st.store()
-        del st, p64
+        del st, c64, p64
+        torch.cuda.empty_cache()
     rate64 = args.members * k64 / (t64 / 1e3)
     # the batch (mixed precision)
     for key in sorted(set(shapes)):
         plans[key] = plan(key[0], key[1], hp.HP_MIXED)
         if not args.no_autotune:
             plans[key].autotune()
-    states = []
+    colls = {key: hp.Collision(plans[key], L=L, Gd=Gd3, nD=nD, **CPRM) for key in hybrid_plans}
+    states, member_colls = [], []
     for k, sh in enumerate(shapes):
         st = hp.State(plans[sh])
         U, s_, V, mu = params(k)
         st.init_mf_gauss(U, s_, V, mu, 0.25 * np.eye(3))
         states.append(st)
-    batch = hp.Batch(states)
+        member_colls.append(colls.get(sh))
+    batch = hp.Batch(states, member_colls, persistent=args.persistent)
     batch.step(dt, 'euler', args.warmup)          # warm-up and graph capture
     torch.cuda.synchronize(dev)
     accuracy = None
@@ -586,8 +622,12 @@ def bench_batch(args, rank, world, local):
            'unit': 'member-steps/s', 'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup,
            'ms_per_batch_step': round(ms / args.steps, 3), 'host_wall_s': round(wall, 3),
            'higher_is_better': True, 'dtype': 'f32 (f64 accumulation)', 'data': 'synthetic',
-           'config': {'workload': 'batch of pendulum FP propagation steps (Euler, dt=1e-3)',
-                      'members': args.members, 'shapes': hist, 'distinct_plans': len(plans)},
+           'config': {'workload': 'batch of pendulum FP steps (Euler, dt=1e-3): hybrid steps with the 3-D collision '
+                                  'reset map for the members whose tables fit, plain propagation for the rest',
+                      'members': args.members, 'shapes': hist, 'distinct_plans': len(plans),
+                      'hybrid_members': sum(1 for c in member_colls if c is not None),
+                      'collision_table_gb': round(used / 1e9, 2), 'persistent_plane_pass': args.persistent,
+                      'launch_shapes': 'autotuned per plan' if not args.no_autotune else 'hand-picked'},
            'fp64_per_density_loop': {'value': round(rate64, 2), 'unit': 'member-steps/s', 'steps_each': k64},
            'speedup_vs_fp64_loop': round(rate / rate64, 3),
            'graph_launches': info['graph_launches'], 'concurrent_streams': info['streams'],

@@ -49,7 +49,8 @@ EXPORTS = ['hp_plan_create', 'hp_plan_destroy', 'hp_plan_get_info', 'hp_plan_set
            'hp_fftSO3_real_backward', 'hp_fftSO3_real_prod', 'hp_plan_set_beta_engine', 'hp_plan_tc_errors',
            'hp_collision_lambda', 'hp_collision_omega', 'hp_collision_fcL', 'hp_collision_create_from_tables',
            'hp_state_set_guard', 'hp_set_device_budget', 'hp_device_bytes', 'hp_plan_autotune',
-           'hp_plan_set_tune', 'hp_plan_get_tune', 'hp_tune_cache_save', 'hp_tune_cache_load']
+           'hp_plan_set_tune', 'hp_plan_get_tune', 'hp_tune_cache_save', 'hp_tune_cache_load',
+           'hp_batch_set_persistent']
 
 
 class HPError(RuntimeError):
@@ -165,6 +166,7 @@ def _load():
         'hp_plan_get_tune': [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)],
         'hp_tune_cache_save': [ctypes.c_char_p],
         'hp_tune_cache_load': [ctypes.c_char_p],
+        'hp_batch_set_persistent': [vp, ip],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -737,6 +739,15 @@ def _x_grid_of(x):
     return nd, N // 2, L
 
 
+def collision_count(plan: Plan, d, h, r, theta_t, lambda_max, L) -> int:
+    """Number of colliding attitudes of the collision operator on `plan` (the
+    numR of getLambda_mex), without building any table."""
+    p = _coll_params(plan.ndim, d=d, h=h, r=r, theta_t=theta_t, lambda_max=lambda_max, L=L)
+    n = ctypes.c_int()
+    _check(_lib.hp_collision_lambda(plan.handle, ctypes.byref(p), ctypes.byref(n), None, None, None, HP_HOST))
+    return n.value
+
+
 def getLambda_mex(R, x, d, h, r, theta_t, lambda_max, compact=False):
     """[lambda, indR, PC] = getLambda_mex(R, x, d, h, r, theta_t, lambda_max, false)
     (propagation/discrete/mex/sources/pendulum_reduced_collision/src/mexLambda.cpp):
@@ -814,7 +825,7 @@ class Batch:
     operator (hybrid step).  Members on different plans run concurrently; the
     steps are replayed from a CUDA graph after one warm-up step."""
 
-    def __init__(self, states, collisions=None):
+    def __init__(self, states, collisions=None, persistent: bool = False):
         n = len(states)
         self._states = list(states)
         self._colls = list(collisions) if collisions is not None else [None] * n
@@ -823,6 +834,8 @@ class Batch:
         h = ctypes.c_void_p()
         _check(_lib.hp_batch_create(arr, carr, n, ctypes.byref(h)))
         self._h = h
+        if persistent:
+            _check(_lib.hp_batch_set_persistent(h, 1))
 
     def __del__(self):
         h = getattr(self, '_h', None)

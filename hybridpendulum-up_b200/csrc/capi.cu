@@ -810,6 +810,9 @@ extern "C" int hp_state_set_guard(hp_state* s, int check_every, double mass_rtol
 
 int hp_state_guard_check(hp_state* s, bool force) {
   if (s->guard_every <= 0 || !s->guard_flag) return HP_OK;
+  // inside a batch step whose plane passes are collected the state is not
+  // final yet: the batch checks its guarded members after the step
+  if (hp_plane_collecting()) return HP_OK;
   if (!force && ++s->guard_count % s->guard_every) return HP_OK;
   hp_plan* p = s->plan;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;

@@ -21,6 +21,7 @@
 //   k_plane   : 2-D (k1, k2) work of every remaining term on one k3 plane of a
 //               tile of n-consecutive rows, then out = F0 + a dF (+ acc += b dF).
 // For ndim = 2 the plane pass covers the whole omega grid and k_axis3 is skipped.
+#include <algorithm>
 #include <atomic>
 #include <vector>
 #include "common.cuh"
@@ -231,7 +232,6 @@ template <> const float2* so3d_table<float>(const hp_plan* p) { return p->so3d32
 template <typename T> static constexpr int local_w() { return sizeof(T) == 8 ? 16 : 32; }
 
 // --------------------------------------------------- pass C: plane pass ----
-struct PlaneTile { int m, l, n0, cnt; };
 
 template <typename T> struct PlaneCfg;
 template <> struct PlaneCfg<double> { static constexpr int C = 1; static constexpr int NT = 128; static constexpr int MINB = 2; };
@@ -247,28 +247,24 @@ __device__ __forceinline__ long long row_of(const RowLayout& L, int l, int m, in
 //   [C+2, 2C+2)        P~ rows n0 .. n0+C-1     (ndim = 3)
 //   [2C+2, 3C+2)       A  = FFT2(Y0) + D_2 FFT2(Y2), then FFT_1
 //   [3C+2, 4C+2)       Y1' = FFT_2(Y1), then D_1 FFT_1
+// One tile (tl) on one k3 plane: the body of k_plane, also run by the
+// persistent batched plane pass (k_plane_batch) for tiles of many members.
 template <int N, typename T, bool HAS_P3, typename TIN>
-__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
-                                                  const c2<TIN>* __restrict__ Fev,
-                                                  const c2<T>* __restrict__ P3,
-                                                  const c2<T>* __restrict__ Gl,
-                                                  const double2* __restrict__ F0, double a,
-                                                  double2* __restrict__ out,
-                                                  double2* __restrict__ acc, double bacc,
-                                                  DerivParams prm, c2<T>* __restrict__ out32 = nullptr) {
+__device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile tl, const int k3,
+                                           const c2<TIN>* __restrict__ Fev, const c2<T>* __restrict__ P3,
+                                           const c2<T>* __restrict__ Gl, const double2* __restrict__ F0, double a,
+                                           double2* __restrict__ out, double2* __restrict__ acc, double bacc,
+                                           const DerivParams& prm, c2<T>* __restrict__ out32, unsigned char* smraw) {
   using C = c2<T>;
   constexpr int CT = PlaneCfg<T>::C;
   constexpr int PS = N * (N + 1);
   constexpr int NP = HAS_P3 ? CT : 0;
-  extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   C* sF = sm;
   C* sP = sm + (CT + 2) * PS;
   C* sA = sm + (CT + 2 + NP) * PS;
   C* sY = sm + (CT + 2 + NP + CT) * PS;
 
-  const PlaneTile tl = tiles[blockIdx.x];
-  const int k3 = HAS_P3 ? (int)blockIdx.y : 0;
   const long long pbase = (long long)k3 * N * N;  // plane offset inside a row
   const int tid = threadIdx.x, nth = blockDim.x;
   const T Ll = (T)prm.L;
@@ -527,6 +523,127 @@ __global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(Ro
   }
 }
 
+template <int N, typename T, bool HAS_P3, typename TIN>
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB) k_plane(RowLayout L, const PlaneTile* __restrict__ tiles,
+                                                  const c2<TIN>* __restrict__ Fev,
+                                                  const c2<T>* __restrict__ P3,
+                                                  const c2<T>* __restrict__ Gl,
+                                                  const double2* __restrict__ F0, double a,
+                                                  double2* __restrict__ out,
+                                                  double2* __restrict__ acc, double bacc,
+                                                  DerivParams prm, c2<T>* __restrict__ out32 = nullptr) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  plane_body<N, T, HAS_P3, TIN>(L, tiles[blockIdx.x], HAS_P3 ? (int)blockIdx.y : 0, Fev, P3, Gl, F0, a, out, acc, bacc,
+                                prm, out32, smraw);
+}
+
+// ----------------------------------------- persistent batched plane pass ----
+// The plane passes of several members (3-D plans of one compute precision,
+// any bandlimit and omega grid) in one launch: every (member, tile, k3 plane)
+// is an item of a work queue that the resident blocks drain through an atomic
+// counter, larger grids first, so the uneven members share the GPU without a
+// launch (and a tail) each.
+
+// one grid size of the batched pass as a separate (not inlined) function, so
+// that each keeps its own register allocation
+template <int N, typename T>
+__device__ __noinline__ void plane_item(const PlaneJob& jb, const PlaneTile tl, int k3, unsigned char* smraw) {
+  using C = c2<T>;
+  plane_body<N, T, true, T>(jb.L, tl, k3, (const C*)jb.Fev, (const C*)jb.P3, (const C*)jb.G, jb.F0, jb.a, jb.out,
+                            jb.acc, jb.bacc, jb.prm, (C*)jb.out32, smraw);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(PlaneCfg<T>::NT, PlaneCfg<T>::MINB)
+    k_plane_batch(const PlaneJob* __restrict__ jobs, int njobs, long long nitems, int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ long long s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= nitems) break;
+    int j = 0;
+    while (j + 1 < njobs && jobs[j + 1].item0 <= it) ++j;
+    const PlaneJob& jb = jobs[j];
+    const long long local = it - jb.item0;
+    const PlaneTile tl = jb.tiles[local / jb.N];
+    const int k3 = (int)(local % jb.N);
+    switch (jb.N) {
+      case 8: plane_item<8, T>(jb, tl, k3, smraw); break;
+      case 12: plane_item<12, T>(jb, tl, k3, smraw); break;
+      case 16: plane_item<16, T>(jb, tl, k3, smraw); break;
+      case 20: plane_item<20, T>(jb, tl, k3, smraw); break;
+      case 24: plane_item<24, T>(jb, tl, k3, smraw); break;
+      case 30: plane_item<30, T>(jb, tl, k3, smraw); break;
+      case 32: plane_item<32, T>(jb, tl, k3, smraw); break;
+      default: break;
+    }
+    __syncthreads();   // shared memory and s_item are reused by the next item
+  }
+}
+
+// Plane passes collected instead of launched while a batch step is being
+// assembled (hp_plane_collect_begin / _end, batch.cu).
+static thread_local std::vector<PlaneJob>* g_collect[2] = {nullptr, nullptr};   // [FP32, FP64]
+
+static bool plane_batchable_N(int N) {
+  return N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 30 || N == 32;
+}
+
+void hp_plane_collect_begin(std::vector<PlaneJob>* f32, std::vector<PlaneJob>* f64) {
+  g_collect[0] = f32;
+  g_collect[1] = f64;
+}
+void hp_plane_collect_end() { g_collect[0] = g_collect[1] = nullptr; }
+size_t hp_plane_job_bytes() { return sizeof(PlaneJob); }
+bool hp_plane_collecting() { return g_collect[0] || g_collect[1]; }
+
+template <typename T> static size_t plane_smem_p3(int N) {
+  constexpr int C = PlaneCfg<T>::C;
+  return (size_t)((C + 2) + C + 2 * C) * N * (N + 1) * sizeof(c2<T>);
+}
+size_t hp_plane_batch_smem(int precision, int Nmax) {
+  return precision == HP_FP64 ? plane_smem_p3<double>(Nmax) : plane_smem_p3<float>(Nmax);
+}
+
+// Runs the collected jobs of one precision in one persistent launch.
+// d_jobs: device array of at least jobs.size() entries (filled by the caller);
+// counter: device int.
+// Orders jobs by grid size (largest first) and numbers their queue items.
+void hp_plane_batch_prepare(std::vector<PlaneJob>& jobs) {
+  std::stable_sort(jobs.begin(), jobs.end(), [](const PlaneJob& a, const PlaneJob& b) { return a.N > b.N; });
+  long long it = 0;
+  for (auto& j : jobs) {
+    j.item0 = it;
+    it += (long long)j.ntiles * j.N;
+  }
+}
+
+int hp_plane_batch_launch(int precision, const std::vector<PlaneJob>& jobs, const PlaneJob* d_jobs, int* counter,
+                          cudaStream_t s) {
+  if (jobs.empty()) return HP_OK;
+  long long nitems = 0;
+  int nmax = 0;
+  for (auto& j : jobs) {
+    nitems = std::max(nitems, j.item0 + (long long)j.ntiles * j.N);
+    nmax = std::max(nmax, j.N);
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), s));
+  const size_t smem = hp_plane_batch_smem(precision, nmax);
+  if (precision == HP_FP64) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane_batch<double><<<148 * PlaneCfg<double>::MINB, PlaneCfg<double>::NT, smem, s>>>(d_jobs, (int)jobs.size(),
+                                                                                            nitems, counter);
+  } else {
+    HP_CUDA_TRY(cudaFuncSetAttribute(k_plane_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_plane_batch<float><<<148 * PlaneCfg<float>::MINB, PlaneCfg<float>::NT, smem, s>>>(d_jobs, (int)jobs.size(),
+                                                                                         nitems, counter);
+  }
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 // ------------------------------------------------------------ launcher ----
 template <typename T> static size_t plane_smem(int N, bool p3) {
   const int C = PlaneCfg<T>::C;
@@ -624,6 +741,27 @@ static int run_deriv_N(hp_plan* p, const double2* Fev, const double2* F0, double
     HP_CUDA_TRY(cudaMemcpy(dt, htiles.data(), sizeof(PlaneTile) * htiles.size(), cudaMemcpyHostToDevice));
   }
   const bool p3 = p->ndim == 3;
+  // inside an assembled batch step the plane pass joins the batch's persistent launch
+  std::vector<PlaneJob>* coll = g_collect[sizeof(T) == 8 ? 1 : 0];
+  if (coll && p3 && plane_batchable_N(N) && (Fc || sizeof(T) == 8)) {
+    PlaneJob jb{};
+    jb.L = L;
+    jb.tiles = dt;
+    jb.ntiles = (int)htiles.size();
+    jb.N = N;
+    jb.Fev = Fc ? (const void*)Fc : (const void*)Fev;
+    jb.P3 = P3;
+    jb.G = G;
+    jb.F0 = F0;
+    jb.a = a;
+    jb.out = out;
+    jb.acc = acc;
+    jb.bacc = bacc;
+    jb.out32 = mixed3 ? out32 : nullptr;
+    jb.prm = prm;
+    coll->push_back(jb);
+    return HP_OK;
+  }
   const size_t smem = plane_smem<T>(N, p3);
   dim3 grid((unsigned)htiles.size(), p3 ? N : 1);
   ProfScope _ps(p, "deriv.plane", s);

@@ -163,6 +163,36 @@ struct DerivParams {
   double gs[3];
   double mr[3][3][2];  // MR_i^1_{0 n2}: [n2+1][i][re, im]
 };
+// Persistent batched plane pass (deriv.cu): between hp_plane_collect_begin and
+// _end, the plane passes of 3-D derivative evaluations are recorded as jobs
+// (per compute precision) instead of launched; hp_plane_batch_prepare numbers
+// their work items, hp_plane_batch_launch runs one precision's jobs (copied
+// to d_jobs by the caller) in one persistent launch.
+struct PlaneTile { int m, l, n0, cnt; };   // (m, l) row, rows n0 .. n0+cnt-1 of the plane pass
+struct PlaneJob {
+  RowLayout L;
+  const PlaneTile* tiles;
+  int ntiles, N;
+  const void* Fev;   // compute-precision input (the FP32 copy, or the FP64 state of FP64 plans)
+  const void* P3;
+  const void* G;
+  const double2* F0;
+  double a;
+  double2* out;
+  double2* acc;
+  double bacc;
+  void* out32;
+  DerivParams prm;
+  long long item0;   // first queue item of this job
+};
+void hp_plane_collect_begin(std::vector<PlaneJob>* f32, std::vector<PlaneJob>* f64);
+void hp_plane_collect_end();
+bool hp_plane_collecting();
+void hp_plane_batch_prepare(std::vector<PlaneJob>& jobs);
+size_t hp_plane_job_bytes();
+int hp_plane_batch_launch(int precision, const std::vector<PlaneJob>& jobs, const PlaneJob* d_jobs, int* counter,
+                          cudaStream_t s);
+
 DerivParams hp_model_params(const hp_plan* p);
 // fev32 (mixed 3-D plans, may be null): Feval already converted to FP32 in the
 // [row][omega] layout; out32 (may be null): receives out converted to FP32.

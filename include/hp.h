@@ -376,6 +376,14 @@ int hp_batch_destroy(hp_batch* batch);
 int hp_batch_step(hp_batch* batch, double dt, int method, int nsteps);
 /* graph replays so far and the number of concurrent streams */
 int hp_batch_info(hp_batch* batch, long long* graph_launches, int* concurrent_streams);
+/* Persistent plane pass: with enable != 0 the plane passes of the members that
+ * take plain Euler steps on 3-D plans (2Bx in 8..32) run as one persistent
+ * kernel per round of members, a work queue over (member, tile, k3 plane)
+ * items drained by the resident blocks, larger grids first; a round holds at
+ * most one member per plan, since members of one plan share its workspace.
+ * Hybrid members, other methods and other grids step as before.  The results
+ * are those of the per-member passes.  Off by default. */
+int hp_batch_set_persistent(hp_batch* batch, int enable);
 
 /* ---- statistics: the raw moments of get_stat (propagation/pendulum.m:547-594,
  * pendulum_reduced_hybrid.m:304-351) ----

@@ -1,8 +1,7 @@
 """Batched propagation (members of uneven bandlimit and omega grid, some
 sharing a plan, some hybrid) against each member stepped on its own: the
 batch replays a captured graph of the same kernels, so plain steps must be
-bit-identical and hybrid steps equal to rounding (their forward transform
-accumulates with atomics)."""
+bit-identical; hybrid steps are held to 1e-12 relative L2."""
 import math
 
 import numpy as np
@@ -79,6 +78,31 @@ def test_batch_hybrid_members(hp):
     batch = hp.Batch(members, colls)
     batch.step(1e-3, 'euler', 5)
     for st, r in zip(members, ref):
-        # the forward transform sums beta groups with atomics: equal to rounding
         out = st.store()
         assert np.linalg.norm(out - r) <= 1e-12 * np.linalg.norm(r)
+
+
+def test_persistent_plane_pass_equals_members(hp):
+    """The plane passes of the plain Euler members on 3-D plans run as one
+    persistent work-queue kernel per round of members (one member per plan and
+    round); members of FP32 and FP64 plans, plans shared by several members, a
+    grid outside the persistent kernel's set (2Bx = 4) and a 2-D member step
+    beside them.  Every member ends as when stepped alone."""
+    shapes = [(4, 4, 3, 1), (6, 6, 3, 1), (4, 4, 3, 1), (5, 4, 3, 0), (8, 8, 3, 1), (4, 4, 3, 1), (3, 2, 3, 1),
+              (6, 2, 2, 1), (5, 4, 3, 0)]
+    plans, members = {}, []
+    for k, (B, Bx, nd, prec) in enumerate(shapes):
+        members.append(make_member(hp, B, Bx, nd, prec, 200 + k, plans))
+    ref = []
+    for st in members:
+        F0 = st.store()
+        st.step(1e-3, 'euler', 9)
+        ref.append(st.store())
+        st.load(F0)
+    batch = hp.Batch(members, persistent=True)
+    batch.step(1e-3, 'euler', 5)
+    batch.step(1e-3, 'euler', 4)
+    assert batch.info()['graph_launches'] >= 1
+    for st, r in zip(members, ref):
+        out = st.store()
+        assert np.linalg.norm(out - r) <= 1e-13 * np.linalg.norm(r)
