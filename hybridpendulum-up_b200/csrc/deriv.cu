@@ -91,6 +91,7 @@ template <typename T> __host__ __device__ constexpr size_t local_tile_bytes(int 
 template <typename T, int W, int NDIM, typename TIN>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __restrict__ F,
                                                c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
+                                               const short* __restrict__ tap_src,
                                                const c2<T>* __restrict__ Gx, const c2<T>* __restrict__ sdk,
                                                DerivParams prm) {
   using C = c2<T>;
@@ -127,16 +128,10 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
   for (int e = tid; e < R * 9; e += nth) sw[e] = tap_wr[(size_t)r0 * 9 + e];
   for (int e = tid; e < D; e += nth) sseg[e] = L.seg[(m - L.m_lo) * D + e] - r0;
   // tap t = (l1 - l + 1) * 3 + (n2 + 1) of row r reads group row ssrc[r][t]
-  // (row 0 where the tap has no weight), so the tap loop below has no branches
+  // (row 0 where the tap has no weight, from the plan's table), so the tap
+  // loop below has no branches
   const int am = abs(m), lmax = L.lmax;
-  for (int e = tid; e < R * 9; e += nth) {
-    const char4 q = L.rows[r0 + e / 9];
-    const int t = e % 9, l1 = q.x + t / 3 - 1, n1 = q.z - (t % 3 - 1), an1 = abs(n1);
-    int src = 0;
-    if (l1 >= 0 && l1 <= lmax && am <= l1 && an1 <= l1)
-      src = L.seg[(m - L.m_lo) * D + n1 + lmax] - r0 + l1 - (am > an1 ? am : an1);
-    ssrc[e] = (short)src;
-  }
+  for (int e = tid; e < R * 9; e += nth) ssrc[e] = tap_src[(size_t)r0 * 9 + e];
   __syncthreads();
   const int w = tid % W, rl = tid / W, nrl = nth / W;
   const long long wg = w0 + w;
@@ -277,21 +272,24 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
   // staging; rows outside -l..l are zero-filled).  FP64 input of an FP32 plan:
   // loads in batches of 8 per thread, converted, then stored.
   const int nF = tl.cnt + 2;
+  // element offsets of the tile's output rows in this plane, for S6
+  __shared__ long long s_rb[CT];
+  if (tid < CT) s_rb[tid] = tid < tl.cnt ? row_of(L, tl.l, tl.m, tl.n0 + tid) * L.nx + pbase : 0;
   if constexpr (sizeof(TIN) == sizeof(T)) {
-    const int tot = nF * N * N;
-    for (int e = tid; e < tot; e += nth) {
-      const int sl = e / (N * N), q = e % (N * N);
+    // one source row per loaded plane: its address once, then the plane's
+    // N^2 elements (rows outside -l..l zero-filled)
+    for (int sl = 0; sl < nF; ++sl) {
       const int n = tl.n0 - 1 + sl;
       const bool ok = n >= -tl.l && n <= tl.l;
-      const c2<TIN>* src = ok ? Fev + row_of(L, tl.l, tl.m, n) * L.nx + pbase + q : Fev;
-      cp_async<sizeof(C)>(sF + sl * PS + (q / N) * (N + 1) + q % N, src, ok);
+      const c2<TIN>* src = ok ? Fev + row_of(L, tl.l, tl.m, n) * L.nx + pbase : Fev;
+      C* dst = sF + sl * PS;
+      for (int q = tid; q < N * N; q += nth) cp_async<sizeof(C)>(dst + (q / N) * (N + 1) + q % N, src + (ok ? q : 0), ok);
     }
     if (HAS_P3) {
-      const int totp = tl.cnt * N * N;
-      for (int e = tid; e < totp; e += nth) {
-        const int sl = e / (N * N), q = e % (N * N);
-        cp_async<sizeof(C)>(sP + sl * PS + (q / N) * (N + 1) + q % N,
-                            P3 + row_of(L, tl.l, tl.m, tl.n0 + sl) * L.nx + pbase + q, true);
+      for (int sl = 0; sl < tl.cnt; ++sl) {
+        const c2<T>* src = P3 + row_of(L, tl.l, tl.m, tl.n0 + sl) * L.nx + pbase;
+        C* dst = sP + sl * PS;
+        for (int q = tid; q < N * N; q += nth) cp_async<sizeof(C)>(dst + (q / N) * (N + 1) + q % N, src + q, true);
       }
     }
     cp_async_wait_all();
@@ -492,7 +490,7 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
         gi[u] = -1;
         if (e < tot) {
           const int c = e / (N * N), q = e % (N * N);
-          gi[u] = row_of(L, tl.l, tl.m, tl.n0 + c) * L.nx + pbase + q;
+          gi[u] = s_rb[c] + q;
           g[u] = Gl[gi[u]];
           f0[u] = F0 ? F0[gi[u]] : make_double2(0.0, 0.0);
           if (acc) ac[u] = acc[gi[u]];
@@ -662,10 +660,12 @@ static int local_w_launch(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* G
   ProfScope _ps(p, "deriv.local", s);
   if (p->ndim == 3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), p->tap_src, Gx,
+                                                   so3d_table<T>(p), prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), p->tap_src, Gx,
+                                                   so3d_table<T>(p), prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;

@@ -26,7 +26,11 @@ static int smem_limit();
 // points, each block holding every row's blk values contiguously,
 // [w / blk][row][w % blk].  One synthesis batch (blk = P omega points) then
 // reads a single contiguous run of nrows * P values, and the rows of one
-// (m, n) pair (consecutive in l) sit P values apart.
+// (m, n) pair (consecutive in l) sit P values apart.  FP64 synthesis reads
+// this layout (B = 15, 32^3: 9.0 ms per synthesis against 10.0 from
+// [row][omega], while the blocked omega-FFT stores cost 0.35 ms more); FP32
+// synthesis reads [row][omega] (the same 2.85 ms either way, and the blocked
+// stores would cost 0.5 ms more).
 __host__ __device__ __forceinline__ long long omega_block_index(long long w, long long row, long long nrows, int blk) {
   return (w / blk * nrows + row) * blk + w % blk;
 }
@@ -167,10 +171,11 @@ __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
 }
 
 // Block = (group of NB consecutive beta indices, range of omega points), the
-// (2l+1)-weighted d values of its betas resident in shared memory.  Input rows
-// are read in the omega-blocked layout [w / P][row][w % P] (omega_block_index):
-// one batch of P omega points is one contiguous run of nrows * P values, the
-// rows of an (m, n) pair P values apart, and the P points of a row on
+// (2l+1)-weighted d values of its betas resident in shared memory.  Input
+// element (row s, omega point w) sits, for FP64, in the omega-blocked layout
+// [w / P][row][w % P] (omega_block_index: one batch is one contiguous run of
+// nrows * P values, the rows of an (m, n) pair P values apart) and, for FP32,
+// in [row][omega] (rows nx values apart).  The P points of a row sit on
 // consecutive lanes; the per-(omega, beta) intermediates G -> H live in shared
 // memory as [bb][m][q][p].
 // GD: the (2l+1) d table of the block's betas is read from a global table
@@ -185,6 +190,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
     k_synth(RowLayout L, const c2<T>* __restrict__ Fp, const T* __restrict__ wig, const int2* __restrict__ pairs,
             void* __restrict__ fout, int nbatch) {
   static_assert(P % PT == 0, "PT divides P");
+  constexpr bool BLOCKED = sizeof(T) == 8;   // input layout (see above)
   using C = c2<T>;
   constexpr int NB2 = 2 * B, lmax = B - 1, D = 2 * lmax + 1;
   constexpr int NM = CPLX ? D : B;
@@ -243,8 +249,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
 #pragma unroll
         for (int pt = 0; pt < PT; ++pt) acc[bb][pt] = czero<C>();
       if (w0 + p0 < nx) {
-        // the batch's block of the omega-blocked input; rows P values apart
-        const C* src = Fp + ((size_t)(w0 / P) * nrows + s) * P + p0;
+        // row s at the item's first omega point; rows rs values apart
+        const size_t rs = BLOCKED ? (size_t)P : (size_t)nx;
+        const C* src = BLOCKED ? Fp + ((size_t)(w0 / P) * nrows + s) * P + p0 : Fp + (size_t)s * nx + w0 + p0;
         const T* dsrc = sd + (size_t)s * NB;
         // a vector load per row where the PT points are all inside the grid
         const bool full = w0 + p0 + PT <= nx;
@@ -260,19 +267,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
                 if (ok && full) {
 #pragma unroll
                   for (int h = 0; h < PT / 2; ++h) {
-                    const float4 w4 = *reinterpret_cast<const float4*>(src + (size_t)(j0 + u) * P + 2 * h);
+                    const float4 w4 = *reinterpret_cast<const float4*>(src + (size_t)(j0 + u) * rs + 2 * h);
                     v[u][2 * h] = mk(w4.x, w4.y);
                     v[u][2 * h + 1] = mk(w4.z, w4.w);
                   }
                 } else {
 #pragma unroll
                   for (int pt = 0; pt < PT; ++pt)
-                    v[u][pt] = (ok && w0 + p0 + pt < nx) ? src[(size_t)(j0 + u) * P + pt] : czero<C>();
+                    v[u][pt] = (ok && w0 + p0 + pt < nx) ? src[(size_t)(j0 + u) * rs + pt] : czero<C>();
                 }
               } else {
 #pragma unroll
                 for (int pt = 0; pt < PT; ++pt)
-                  v[u][pt] = (ok && (PT == 1 || w0 + p0 + pt < nx)) ? src[(size_t)(j0 + u) * P + pt] : czero<C>();
+                  v[u][pt] = (ok && (PT == 1 || w0 + p0 + pt < nx)) ? src[(size_t)(j0 + u) * rs + pt] : czero<C>();
               }
             }
 #pragma unroll
@@ -521,9 +528,11 @@ template <int B, typename T, bool CPLX> struct SynthCfg {
   static constexpr int P = pick_p();
 };
 
-// Omega block of the synthesis input (P of the synthesis configuration).
+// Omega block of the synthesis input (P of the synthesis configuration) for
+// FP64 synthesis; 0 (the [row][omega] layout) for FP32.
 template <typename T, bool CPLX>
 static int synth_block(const hp_plan* p) {
+  if (sizeof(T) == 4) return 0;
   switch (p->B) {
 #define X(b) case b: return SynthCfg<b, T, CPLX>::P;
     X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(15) X(16) X(20) X(24) X(30) X(32)
@@ -661,14 +670,16 @@ static int synth_any(hp_plan* p, const c2<T>* Fp, void* f, cudaStream_t s) {
 }
 
 
-// Inverse omega FFT of every row into the omega-blocked synthesis input (a
-// plan workspace sized for whole blocks), then the synthesis.
+// Inverse omega FFT of every row into the synthesis input (a plan workspace;
+// omega-blocked and sized for whole blocks for FP64, [row][omega] for FP32),
+// then the synthesis.
 template <typename Tin, typename T>
 static int backward_rows(hp_plan* p, const c2<Tin>* Fint, void* f, int complex_out, cudaStream_t s) {
   using C = c2<T>;
   int st = HP_OK;
   const int blk = complex_out ? synth_block<T, true>(p) : synth_block<T, false>(p);
-  const size_t fb = sizeof(C) * (size_t)p->nrows * ((p->nx + blk - 1) / blk * blk);
+  const long long nxb = blk ? (p->nx + blk - 1) / blk * blk : p->nx;
+  const size_t fb = sizeof(C) * (size_t)p->nrows * nxb;
   C* t1 = (C*)p->ws_get("tf.t1", fb, &st);
   if (st) return st;
   st = omega_fft_any<Tin, T>(p, Fint, t1, true, s, blk);
