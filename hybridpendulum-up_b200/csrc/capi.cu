@@ -239,7 +239,6 @@ extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
   hp_dev_free(p->rows); hp_dev_free(p->seg); hp_dev_free(p->wig64); hp_dev_free(p->wig32); hp_dev_free(p->wfull);
   hp_dev_free(p->qw); hp_dev_free(p->cg1); hp_dev_free(p->tap_wr); hp_dev_free(p->tap_wr32);
-  hp_dev_free(p->tap_src);
   p->prof_on = false;
   prof_collect(p);
   for (auto& kv : p->ws) hp_dev_free(kv.second.p);

@@ -91,7 +91,6 @@ template <typename T> __host__ __device__ constexpr size_t local_tile_bytes(int 
 template <typename T, int W, int NDIM, typename TIN>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __restrict__ F,
                                                c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
-                                               const short* __restrict__ tap_src,
                                                const c2<T>* __restrict__ Gx, const c2<T>* __restrict__ sdk,
                                                DerivParams prm) {
   using C = c2<T>;
@@ -128,10 +127,18 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
   for (int e = tid; e < R * 9; e += nth) sw[e] = tap_wr[(size_t)r0 * 9 + e];
   for (int e = tid; e < D; e += nth) sseg[e] = L.seg[(m - L.m_lo) * D + e] - r0;
   // tap t = (l1 - l + 1) * 3 + (n2 + 1) of row r reads group row ssrc[r][t]
-  // (row 0 where the tap has no weight, from the plan's table), so the tap
-  // loop below has no branches
+  // (row 0 where the tap has no weight), so the tap loop below has no branches
+  // (computed here from the row table: fewer bytes per block than a stored
+  // [row][9] index table, which measured slower with the 16-point FP64 tiles)
   const int am = abs(m), lmax = L.lmax;
-  for (int e = tid; e < R * 9; e += nth) ssrc[e] = tap_src[(size_t)r0 * 9 + e];
+  for (int e = tid; e < R * 9; e += nth) {
+    const char4 q = L.rows[r0 + e / 9];
+    const int t = e % 9, l1 = q.x + t / 3 - 1, n1 = q.z - (t % 3 - 1), an1 = abs(n1);
+    int src = 0;
+    if (l1 >= 0 && l1 <= lmax && am <= l1 && an1 <= l1)
+      src = L.seg[(m - L.m_lo) * D + n1 + lmax] - r0 + l1 - (am > an1 ? am : an1);
+    ssrc[e] = (short)src;
+  }
   __syncthreads();
   const int w = tid % W, rl = tid / W, nrl = nth / W;
   const long long wg = w0 + w;
@@ -660,12 +667,10 @@ static int local_w_launch(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* G
   ProfScope _ps(p, "deriv.local", s);
   if (p->ndim == 3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), p->tap_src, Gx,
-                                                   so3d_table<T>(p), prm);
+    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), p->tap_src, Gx,
-                                                   so3d_table<T>(p), prm);
+    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;

@@ -58,7 +58,6 @@ struct hp_plan {
   hp_model model{};
   double* tap_wr = nullptr;  // [row][9] real gravity tap weights, tap (l1-l+1)*3 + (n2+1)
   float* tap_wr32 = nullptr;
-  short* tap_src = nullptr;  // [row][9] source row of each tap, relative to the row's m group
   double2 mr1[3][3] = {};    // MR_i^1_{0 n2} of the model: [n2+1][i]
   double* den_mR = nullptr;  // [2][(2B)^3] density-side gravity multipliers (pendulum_reduced_den)
   // attitude diffusion sum_ij G1_ij F^l u_i^T u_j^T of the gyro-bias model:

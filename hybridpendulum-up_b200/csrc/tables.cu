@@ -117,30 +117,22 @@ __global__ void k_cg1(int lmax, double* cg1) {
 // weight factors into a real part per tap, stored here as
 // tap_wr[row*9 + (l1-l+1)*3 + (n2+1)] (zero where the source row does not
 // exist), and the model's MR_i^1_{0 n2}, applied per omega point.
-// tap_src (may be null): the tap's source row F^{l1}_{m, n-n2} as an offset
-// from the first row of the m group (0 where the tap has no weight), the
-// index the gravity pass reads its group tile at.
 template <typename T>
-__global__ void k_gravity_taps(RowLayout L, const double* __restrict__ cg1, T* __restrict__ tap_wr,
-                               short* __restrict__ tap_src) {
+__global__ void k_gravity_taps(RowLayout L, const double* __restrict__ cg1, T* __restrict__ tap_wr) {
   const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (r >= L.nrows) return;
-  const int lmax = L.lmax, D = 2 * lmax + 1;
+  const int lmax = L.lmax;
   const char4 q = L.rows[r];
-  const int l = q.x, m = q.y, n = q.z, am = abs(m);
-  const int r0 = L.seg[(m - L.m_lo) * D];
+  const int l = q.x, m = q.y, n = q.z;
   for (int t = 0; t < 9; ++t) {
-    const int l1 = l + t / 3 - 1, n2 = t % 3 - 1, n1 = n - n2, an1 = abs(n1);
+    const int l1 = l + t / 3 - 1, n2 = t % 3 - 1, n1 = n - n2;
     double w = 0.0;
-    int src = 0;
-    if (l1 >= 0 && l1 <= lmax && am <= l1 && an1 <= l1) {
+    if (l1 >= 0 && l1 <= lmax && abs(m) <= l1 && abs(n1) <= l1) {
       const double cm = cg1[cg1_index(lmax, l1, l - l1, m, 0)];
       const double cn = cg1[cg1_index(lmax, l1, l - l1, n, n2)];
       w = (2.0 * l1 + 1.0) * 3.0 / (2.0 * l + 1.0) * cm * cn;
-      src = L.seg[(m - L.m_lo) * D + n1 + lmax] - r0 + l1 - (am > an1 ? am : an1);
     }
     tap_wr[r * 9 + t] = (T)w;
-    if (tap_src) tap_src[r * 9 + t] = (short)src;
   }
 }
 
@@ -286,10 +278,9 @@ int hp_build_gravity_taps(hp_plan* p) {
   if (p->tap_wr) return HP_OK;
   HP_CUDA_TRY(hp_dev_alloc(&p->tap_wr, sizeof(double) * 9 * p->nrows));
   HP_CUDA_TRY(hp_dev_alloc(&p->tap_wr32, sizeof(float) * 9 * p->nrows));
-  HP_CUDA_TRY(hp_dev_alloc((void**)&p->tap_src, sizeof(short) * 9 * p->nrows));
   const unsigned g = (unsigned)((p->nrows + 127) / 128);
-  k_gravity_taps<double><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr, p->tap_src);
-  k_gravity_taps<float><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr32, nullptr);
+  k_gravity_taps<double><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr);
+  k_gravity_taps<float><<<g, 128, 0, p->stream>>>(p->layout(), p->cg1, p->tap_wr32);
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
 }

@@ -35,60 +35,79 @@ __host__ __device__ __forceinline__ long long omega_block_index(long long w, lon
   return (w / blk * nrows + row) * blk + w % blk;
 }
 
-// 2-D FFT over (k1, k2) of every (row, k3) plane; one block per (row, k3).
+// Planes per block of k_wplane: enough that the N FFTs of each pass of every
+// plane give the 128 threads one FFT each, within 64 KB of shared memory.
+template <int N, typename T> __host__ __device__ constexpr int wplane_ppb() {
+  constexpr int want = 128 / N > 1 ? 128 / N : 1;
+  constexpr int fit = (int)((64 * 1024) / ((size_t)N * (N + 1) * sizeof(c2<T>)));
+  return want < fit ? want : (fit > 1 ? fit : 1);
+}
+
+// 2-D FFT over (k1, k2) of every (row, k3) plane; PPB consecutive planes (one
+// contiguous run of PPB N^2 values) per block.
 // blk > 0: the output goes to the omega-blocked layout of the synthesis input
 // (see omega_block_index), plane pl holding omega points pl_w0 .. pl_w0 + N^2 of
-// row pl / planes_per_row.
+// row pl / planes_per_row.  in may equal out (a block reads all of its planes
+// before it writes).
 template <int N, typename Tin, typename T, bool INV>
 __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, c2<T>* __restrict__ out,
                                                 long long nplanes, T scale, int blk = 0, long long nrows = 0,
                                                 int planes_per_row = 1) {
   using C = c2<T>;
+  constexpr int PPB = wplane_ppb<N, T>();
+  constexpr int PS = N * (N + 1);
   extern __shared__ __align__(16) unsigned char smraw[];
-  C* sm = reinterpret_cast<C*>(smraw);   // [N][N+1]
-  const long long pl = blockIdx.x;
-  if (pl >= nplanes) return;
-  const c2<Tin>* src = in + pl * N * N;
-  for (int e0 = threadIdx.x; e0 < N * N; e0 += 4 * blockDim.x) {
+  C* sm = reinterpret_cast<C*>(smraw);   // [PPB][N][N+1]
+  const long long pl0 = (long long)blockIdx.x * PPB;
+  if (pl0 >= nplanes) return;
+  const int np = (int)min((long long)PPB, nplanes - pl0);
+  const int tot = np * N * N;
+  const c2<Tin>* src = in + pl0 * N * N;
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
     C v[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int e = e0 + u * blockDim.x;
-      v[u] = e < N * N ? cvt<C, c2<Tin>>(src[e]) : czero<C>();
+      v[u] = e < tot ? cvt<C, c2<Tin>>(src[e]) : czero<C>();
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int e = e0 + u * blockDim.x;
-      if (e < N * N) sm[(e / N) * (N + 1) + e % N] = v[u];
+      if (e < tot) sm[(e / (N * N)) * PS + ((e / N) % N) * (N + 1) + e % N] = v[u];
     }
   }
   __syncthreads();
-  for (int k2 = threadIdx.x; k2 < N; k2 += blockDim.x) {
+  for (int it = threadIdx.x; it < np * N; it += blockDim.x) {
+    C* row = sm + (it / N) * PS + (it % N) * (N + 1);
     C x[N];
 #pragma unroll
-    for (int j = 0; j < N; ++j) x[j] = sm[k2 * (N + 1) + j];
+    for (int j = 0; j < N; ++j) x[j] = row[j];
     fft<N, INV>(x);
 #pragma unroll
-    for (int j = 0; j < N; ++j) sm[k2 * (N + 1) + j] = x[j];
+    for (int j = 0; j < N; ++j) row[j] = x[j];
   }
   __syncthreads();
-  for (int k1 = threadIdx.x; k1 < N; k1 += blockDim.x) {
+  for (int it = threadIdx.x; it < np * N; it += blockDim.x) {
+    C* col = sm + (it / N) * PS + it % N;
     C x[N];
 #pragma unroll
-    for (int j = 0; j < N; ++j) x[j] = sm[j * (N + 1) + k1];
+    for (int j = 0; j < N; ++j) x[j] = col[j * (N + 1)];
     fft<N, INV>(x);
 #pragma unroll
-    for (int j = 0; j < N; ++j) sm[j * (N + 1) + k1] = scale * x[j];
+    for (int j = 0; j < N; ++j) col[j * (N + 1)] = scale * x[j];
   }
   __syncthreads();
   if (blk > 0) {
-    const long long row = pl / planes_per_row, w0 = (pl % planes_per_row) * (long long)(N * N);
-    for (int e = threadIdx.x; e < N * N; e += blockDim.x)
-      out[omega_block_index(w0 + e, row, nrows, blk)] = sm[(e / N) * (N + 1) + e % N];
+    for (int e = threadIdx.x; e < tot; e += blockDim.x) {
+      const long long pl = pl0 + e / (N * N);
+      const int q = e % (N * N);
+      const long long row = pl / planes_per_row, w0 = (pl % planes_per_row) * (long long)(N * N);
+      out[omega_block_index(w0 + q, row, nrows, blk)] = sm[(e / (N * N)) * PS + (q / N) * (N + 1) + q % N];
+    }
     return;
   }
-  C* dst = out + pl * N * N;
-  for (int e = threadIdx.x; e < N * N; e += blockDim.x) dst[e] = sm[(e / N) * (N + 1) + e % N];
+  C* dst = out + pl0 * N * N;
+  for (int e = threadIdx.x; e < tot; e += blockDim.x) dst[e] = sm[(e / (N * N)) * PS + ((e / N) % N) * (N + 1) + e % N];
 }
 
 // 1-D FFT along the last omega axis (stride N^2) of a [row][N^3] array.
@@ -440,15 +459,17 @@ static int omega_fft(hp_plan* p, const c2<Tin>* in, c2<T>* out, bool inv, cudaSt
   const T scale = inv ? (T)1 / (T)p->nx : (T)1;
   const int ppr = p->ndim == 3 ? N : 1;
   const long long nplanes = p->nrows * ppr;
-  const size_t smem = sizeof(c2<T>) * N * (N + 1);
+  constexpr int PPB = wplane_ppb<N, T>();
+  const size_t smem = sizeof(c2<T>) * PPB * N * (N + 1);
+  const unsigned nblk = (unsigned)((nplanes + PPB - 1) / PPB);
   auto plane = [&](T sc) -> int {
     ProfScope _ps(p, "tf.wplane", s);
     if (inv) {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_wplane<N, Tin, T, true><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
+      k_wplane<N, Tin, T, true><<<nblk, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
     } else {
       HP_CUDA_TRY(cudaFuncSetAttribute(k_wplane<N, Tin, T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      k_wplane<N, Tin, T, false><<<(unsigned)nplanes, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
+      k_wplane<N, Tin, T, false><<<nblk, 128, smem, s>>>(in, out, nplanes, sc, blk, p->nrows, ppr);
     }
     HP_CUDA_TRY(cudaGetLastError());
     return HP_OK;
