@@ -77,9 +77,10 @@ __global__ void __launch_bounds__(128) k_axis3(RowLayout L, const c2<TIN>* __res
 }
 
 // ------------------------------------------------ pass B: gravity + noise ----
-// Block = one m group x W consecutive omega points.  The group's rows and
-// their real tap weights are staged once in shared memory (taps stay inside
-// the group because the gravity multiplier has m2 = 0); a warp handles one
+// Block = one m group x cpb chunks of W consecutive omega points.  The
+// group's real tap weights and tap sources are staged once per block, its
+// rows once per chunk, in shared memory (taps stay inside the group because
+// the gravity multiplier has m2 = 0); a warp handles one
 // output row at a time, lanes are omega points, so the tap loop is
 // warp-uniform and reads shared memory only.  Per omega point the model part
 // of the weights folds into nu[n2] = -i sum_i D_i gs_i MR_i^1_{0 n2}, so
@@ -92,7 +93,7 @@ template <typename T, int W, int NDIM, typename TIN>
 __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __restrict__ F,
                                                c2<T>* __restrict__ G, const T* __restrict__ tap_wr,
                                                const c2<T>* __restrict__ Gx, const c2<T>* __restrict__ sdk,
-                                               DerivParams prm) {
+                                               DerivParams prm, int cpb) {
   using C = c2<T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int D = 2 * L.lmax + 1;
@@ -106,30 +107,13 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
   const int r0 = L.seg[(m - L.m_lo) * D];
   const int r1 = (m + 1 <= L.lmax) ? L.seg[(m + 1 - L.m_lo) * D] : (int)L.nrows;
   const int R = r1 - r0;
-  const long long w0 = (long long)blockIdx.x * W;
   const int tid = threadIdx.x, nth = blockDim.x;
-  // group rows staged with 8 loads in flight per thread (asynchronous copies
-  // into the tile measured no faster here)
-  for (int e0 = tid; e0 < R * W; e0 += 8 * nth) {
-    C v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * nth;
-      const int r = e / W, w = e % W;
-      v[u] = (e < R * W && w0 + w < L.nx) ? cvt<C, c2<TIN>>(F[(size_t)(r0 + r) * L.nx + w0 + w]) : czero<C>();
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int e = e0 + u * nth;
-      if (e < R * W) tile[e] = v[u];
-    }
-  }
+  // per block, once for its cpb omega chunks: the group's tap weights and tap
+  // sources
   for (int e = tid; e < R * 9; e += nth) sw[e] = tap_wr[(size_t)r0 * 9 + e];
   for (int e = tid; e < D; e += nth) sseg[e] = L.seg[(m - L.m_lo) * D + e] - r0;
   // tap t = (l1 - l + 1) * 3 + (n2 + 1) of row r reads group row ssrc[r][t]
   // (row 0 where the tap has no weight), so the tap loop below has no branches
-  // (computed here from the row table: fewer bytes per block than a stored
-  // [row][9] index table, which measured slower with the 16-point FP64 tiles)
   const int am = abs(m), lmax = L.lmax;
   for (int e = tid; e < R * 9; e += nth) {
     const char4 q = L.rows[r0 + e / 9];
@@ -139,83 +123,106 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
       src = L.seg[(m - L.m_lo) * D + n1 + lmax] - r0 + l1 - (am > an1 ? am : an1);
     ssrc[e] = (short)src;
   }
-  __syncthreads();
-  const int w = tid % W, rl = tid / W, nrl = nth / W;
-  const long long wg = w0 + w;
-  if (wg >= L.nx) return;
   const int N = L.N;
   const T tp = (T)(2.0 * M_PI / prm.L);
-  T d1[NDIM], dd[NDIM];
-  {
-    long long ww = wg;
+  const int w = tid % W, rl = tid / W, nrl = nth / W;
+  const long long nchunks = (L.nx + W - 1) / W;
+  const long long ch0 = (long long)blockIdx.x * cpb;
+  const long long ch1 = ch0 + cpb < nchunks ? ch0 + cpb : nchunks;
+  for (long long ch = ch0; ch < ch1; ++ch) {
+    const long long w0 = ch * W;
+    __syncthreads();   // the previous chunk's reads of the tile are done
+    // group rows staged with 8 loads in flight per thread (asynchronous copies
+    // into the tile measured no faster here)
+    for (int e0 = tid; e0 < R * W; e0 += 8 * nth) {
+      C v[8];
 #pragma unroll
-    for (int a = 0; a < NDIM; ++a) {
-      const int k = (int)(ww % N);
-      ww /= N;
-      d1[a] = tp * (T)kappa_first(k, N);
-      dd[a] = tp * (T)kappa_diag(k, N);
-    }
-  }
-  T noise = 0;
-#pragma unroll
-  for (int i = 0; i < NDIM; ++i)
-#pragma unroll
-    for (int j = 0; j < NDIM; ++j)
-      noise -= (T)prm.G[i * 3 + j] * ((i == j) ? dd[i] * dd[i] : d1[i] * d1[j]);
-  C nu[3];  // -i sum_i d1_i gs_i MR_i^1_{0 n2}
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    T mx = 0, my = 0;
-#pragma unroll
-    for (int i = 0; i < NDIM; ++i) {
-      const T s = d1[i] * (T)prm.gs[i];
-      mx += s * (T)prm.mr[q][i][0];
-      my += s * (T)prm.mr[q][i][1];
-    }
-    nu[q].x = my;
-    nu[q].y = -mx;
-  }
-  for (int r = rl; r < R; r += nrl) {
-    const C f0 = tile[r * W + w];
-    T ax = noise * f0.x, ay = noise * f0.y;
-#pragma unroll
-    for (int n2o = 0; n2o < 3; ++n2o) {
-      T sx = 0, sy = 0;
-#pragma unroll
-      for (int l1o = 0; l1o < 3; ++l1o) {
-        const int t = r * 9 + l1o * 3 + n2o;
-        const T wt = sw[t];
-        const C fs = tile[ssrc[t] * W + w];
-        sx = fma(wt, fs.x, sx);
-        sy = fma(wt, fs.y, sy);
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * nth;
+        const int r = e / W, ww = e % W;
+        v[u] = (e < R * W && w0 + ww < L.nx) ? cvt<C, c2<TIN>>(F[(size_t)(r0 + r) * L.nx + w0 + ww]) : czero<C>();
       }
-      ax += nu[n2o].x * sx - nu[n2o].y * sy;
-      ay += nu[n2o].x * sy + nu[n2o].y * sx;
-    }
-    if (sdk) {  // attitude diffusion: sum_o K^l[n][n+o-2] F^l_{m, n+o-2} (gyro-bias model)
-      const char4 q = L.rows[r0 + r];
-      const int l = q.x, n = q.z;
-      const c2<T>* kw = sdk + (size_t)(r0 + r) * 5;
 #pragma unroll
-      for (int o = 0; o < 5; ++o) {
-        const int k = n + o - 2;
-        if (k < -l || k > l) continue;
-        const int ak = abs(k);
-        const C fs = tile[(sseg[k + lmax] - (am > ak ? am : ak) + l) * W + w];
-        const C wk = kw[o];
-        ax += wk.x * fs.x - wk.y * fs.y;
-        ay += wk.x * fs.y + wk.y * fs.x;
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * nth;
+        if (e < R * W) tile[e] = v[u];
       }
     }
-    if (Gx) {  // density-side gravity term (density-gravity models)
-      const C gx = Gx[(size_t)(r0 + r) * L.nx + wg];
-      ax += gx.x;
-      ay += gx.y;
+    __syncthreads();
+    const long long wg = w0 + w;
+    if (wg >= L.nx) continue;
+    T d1[NDIM], dd[NDIM];
+    {
+      long long ww = wg;
+#pragma unroll
+      for (int a = 0; a < NDIM; ++a) {
+        const int k = (int)(ww % N);
+        ww /= N;
+        d1[a] = tp * (T)kappa_first(k, N);
+        dd[a] = tp * (T)kappa_diag(k, N);
+      }
     }
-    C o;
-    o.x = ax;
-    o.y = ay;
-    G[(size_t)(r0 + r) * L.nx + wg] = o;
+    T noise = 0;
+#pragma unroll
+    for (int i = 0; i < NDIM; ++i)
+#pragma unroll
+      for (int j = 0; j < NDIM; ++j)
+        noise -= (T)prm.G[i * 3 + j] * ((i == j) ? dd[i] * dd[i] : d1[i] * d1[j]);
+    C nu[3];  // -i sum_i d1_i gs_i MR_i^1_{0 n2}
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      T mx = 0, my = 0;
+#pragma unroll
+      for (int i = 0; i < NDIM; ++i) {
+        const T s = d1[i] * (T)prm.gs[i];
+        mx += s * (T)prm.mr[q][i][0];
+        my += s * (T)prm.mr[q][i][1];
+      }
+      nu[q].x = my;
+      nu[q].y = -mx;
+    }
+    for (int r = rl; r < R; r += nrl) {
+      const C f0 = tile[r * W + w];
+      T ax = noise * f0.x, ay = noise * f0.y;
+#pragma unroll
+      for (int n2o = 0; n2o < 3; ++n2o) {
+        T sx = 0, sy = 0;
+#pragma unroll
+        for (int l1o = 0; l1o < 3; ++l1o) {
+          const int t = r * 9 + l1o * 3 + n2o;
+          const T wt = sw[t];
+          const C fs = tile[ssrc[t] * W + w];
+          sx = fma(wt, fs.x, sx);
+          sy = fma(wt, fs.y, sy);
+        }
+        ax += nu[n2o].x * sx - nu[n2o].y * sy;
+        ay += nu[n2o].x * sy + nu[n2o].y * sx;
+      }
+      if (sdk) {  // attitude diffusion: sum_o K^l[n][n+o-2] F^l_{m, n+o-2} (gyro-bias model)
+        const char4 q = L.rows[r0 + r];
+        const int l = q.x, n = q.z;
+        const c2<T>* kw = sdk + (size_t)(r0 + r) * 5;
+#pragma unroll
+        for (int o = 0; o < 5; ++o) {
+          const int k = n + o - 2;
+          if (k < -l || k > l) continue;
+          const int ak = abs(k);
+          const C fs = tile[(sseg[k + lmax] - (am > ak ? am : ak) + l) * W + w];
+          const C wk = kw[o];
+          ax += wk.x * fs.x - wk.y * fs.y;
+          ay += wk.x * fs.y + wk.y * fs.x;
+        }
+      }
+      if (Gx) {  // density-side gravity term (density-gravity models)
+        const C gx = Gx[(size_t)(r0 + r) * L.nx + wg];
+        ax += gx.x;
+        ay += gx.y;
+      }
+      C o;
+      o.x = ax;
+      o.y = ay;
+      G[(size_t)(r0 + r) * L.nx + wg] = o;
+    }
   }
 }
 
@@ -663,14 +670,18 @@ template <typename T, int W, typename TIN>
 static int local_w_launch(hp_plan* p, const c2<TIN>* F, c2<T>* G, const c2<T>* Gx, const DerivParams& prm,
                           cudaStream_t s) {
   const size_t lsm = local_smem<T>(p, W);
-  dim3 grid((unsigned)((p->nx + W - 1) / W), (unsigned)p->nm);
+  // omega chunks per block: the per-block staging of the tap tables amortised
+  // over several chunks while about twelve blocks per SM remain
+  const long long nchunks = (p->nx + W - 1) / W;
+  const int cpb = (int)std::max(1LL, std::min(64LL, nchunks * p->nm / (148LL * 12)));
+  dim3 grid((unsigned)((nchunks + cpb - 1) / cpb), (unsigned)p->nm);
   ProfScope _ps(p, "deriv.local", s);
   if (p->ndim == 3) {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 3, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    k_local<T, W, 3, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm, cpb);
   } else {
     HP_CUDA_TRY(cudaFuncSetAttribute(k_local<T, W, 2, TIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
-    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm);
+    k_local<T, W, 2, TIN><<<grid, 256, lsm, s>>>(p->layout(), F, G, tap_table<T>(p), Gx, so3d_table<T>(p), prm, cpb);
   }
   HP_CUDA_TRY(cudaGetLastError());
   return HP_OK;
