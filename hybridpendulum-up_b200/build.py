@@ -14,7 +14,11 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, 'libhp.so')
-SOURCES = ['tables.cu', 'deriv.cu', 'transform.cu', 'prod.cu', 'capi.cu', 'collision.cu', 'adjoint.cu', 'stats.cu', 'init.cu', 'batch.cu', 'real.cu', 'tc_beta.cu', 'tune.cu']
+# the per-bandlimit transform kernels are split over transform_b0..3.cu (B mod 4)
+# so that they compile in parallel; the longest units first
+SOURCES = ['transform_b0.cu', 'transform_b1.cu', 'transform_b2.cu', 'transform_b3.cu', 'deriv.cu', 'adjoint.cu',
+           'transform.cu', 'tables.cu', 'prod.cu', 'capi.cu', 'collision.cu', 'stats.cu', 'init.cu', 'batch.cu',
+           'real.cu', 'tc_beta.cu', 'tune.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
          '-Xptxas', '-warn-spills']

@@ -197,20 +197,11 @@ int axis_md_launch(hp_plan* p, const double2* in, double2* out, int axis, double
 
 int axis_md(hp_plan* p, const double2* in, double2* out, int axis, double coef, cudaStream_t s) {
   switch (p->N) {
-    case 4: return axis_md_launch<4>(p, in, out, axis, coef, s);
-    case 6: return axis_md_launch<6>(p, in, out, axis, coef, s);
-    case 8: return axis_md_launch<8>(p, in, out, axis, coef, s);
-    case 12: return axis_md_launch<12>(p, in, out, axis, coef, s);
-    case 16: return axis_md_launch<16>(p, in, out, axis, coef, s);
-    case 20: return axis_md_launch<20>(p, in, out, axis, coef, s);
-    case 24: return axis_md_launch<24>(p, in, out, axis, coef, s);
-    case 30: return axis_md_launch<30>(p, in, out, axis, coef, s);
-    case 32: return axis_md_launch<32>(p, in, out, axis, coef, s);
-    case 40: return axis_md_launch<40>(p, in, out, axis, coef, s);
-    case 48: return axis_md_launch<48>(p, in, out, axis, coef, s);
-    case 60: return axis_md_launch<60>(p, in, out, axis, coef, s);
+#define X(n) case n: return axis_md_launch<n>(p, in, out, axis, coef, s);
+    HP_FOR_EACH_N(X)
+#undef X
     default:
-      hp_set_error("omega grid size 2Bx not supported");
+      hp_set_error("omega grid size 2Bx not supported (even, 4..64)");
       return HP_ERR_UNSUPPORTED;
   }
 }

@@ -192,25 +192,14 @@ extern "C" int hp_plan_tc_errors(hp_plan* p, int* count) {
   return hp::tc_beta_errors(p, count);
 }
 
-static bool valid_N(int N) {
-  return N == 4 || N == 6 || N == 8 || N == 12 || N == 16 || N == 20 || N == 24 || N == 30 || N == 32 || N == 40 ||
-         N == 48 || N == 60;
-}
-static bool valid_B(int B) {
-  switch (B) {
-    case 2: case 3: case 4: case 5: case 6: case 8: case 10: case 12: case 15: case 16: case 20: case 24: case 30:
-    case 32:
-      return true;
-    default:
-      return false;
-  }
-}
+static bool valid_N(int N) { return N >= 4 && N <= 64 && N % 2 == 0; }
+static bool valid_B(int B) { return B >= 2 && B <= 32; }
 
 extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precision, int symmetry) {
   if (!out) { hp_set_error("plan pointer is null"); return HP_ERR_INVALID; }
   *out = nullptr;
-  if (!valid_B(B)) { hp_set_error("bandlimit B not supported (2,3,4,5,6,8,10,12,15,16,20,24,30,32)"); return HP_ERR_INVALID; }
-  if (!valid_N(2 * Bx)) { hp_set_error("2*Bx must be one of 4,6,8,12,16,20,24,30,32,40,48,60"); return HP_ERR_INVALID; }
+  if (!valid_B(B)) { hp_set_error("bandlimit B must be 2..32"); return HP_ERR_INVALID; }
+  if (!valid_N(2 * Bx)) { hp_set_error("Bx must be 2..32 (omega grids of 4..64 points per axis)"); return HP_ERR_INVALID; }
   if (ndim != 2 && ndim != 3) { hp_set_error("ndim must be 2 or 3"); return HP_ERR_INVALID; }
   if (precision != HP_FP64 && precision != HP_MIXED) { hp_set_error("bad precision"); return HP_ERR_INVALID; }
   if (symmetry != HP_REAL && symmetry != HP_COMPLEX) { hp_set_error("bad symmetry"); return HP_ERR_INVALID; }

@@ -66,11 +66,36 @@ template <> __device__ __forceinline__ double2 cvt<double2, float2>(float2 a) { 
 
 template <typename C> __device__ __forceinline__ C czero() { C r; r.x = 0; r.y = 0; return r; }
 
+// ------------------------------------------------------------ sizes ----
+// Kernels are instantiated per bandlimit B (2..32) and per omega grid size N
+// (even, 4..64; the plane kernels of the derivative for N <= 32).
+#define HP_FOR_EACH_B(X) \
+  X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17) X(18) X(19) X(20) \
+  X(21) X(22) X(23) X(24) X(25) X(26) X(27) X(28) X(29) X(30) X(31) X(32)
+#define HP_FOR_EACH_N_TO_32(X) \
+  X(4) X(6) X(8) X(10) X(12) X(14) X(16) X(18) X(20) X(22) X(24) X(26) X(28) X(30) X(32)
+#define HP_FOR_EACH_N_ABOVE_32(X) \
+  X(34) X(36) X(38) X(40) X(42) X(44) X(46) X(48) X(50) X(52) X(54) X(56) X(58) X(60) X(62) X(64)
+#define HP_FOR_EACH_N(X) HP_FOR_EACH_N_TO_32(X) HP_FOR_EACH_N_ABOVE_32(X)
+
 // ------------------------------------------------------------ twiddles ----
-// W[k] = exp(-2 pi i k / 960); every transform length used here divides 960.
-// Each translation unit holds its own copy (no relocatable device code) and
-// fills it once per device with tw_init() before its first launch.
-constexpr int kTwN = 960;
+// Entries 0..959: W[k] = exp(-2 pi i k / 960), the twiddles of every length
+// that divides 960 (all the 2/3/5 sizes).  Then one section per other length
+// M that an FFT of at most 64 points can need (M <= 64 not dividing 960, even
+// or at most 32): W_M^e, e = 0..M-1.  Each translation unit holds its own copy
+// (no relocatable device code) and fills it once per device with tw_init()
+// before its first launch.
+constexpr int kTw960 = 960;
+constexpr int kTwMaxM = 64;
+__host__ __device__ constexpr bool tw_own_section(int M) {
+  return kTw960 % M != 0 && (M % 2 == 0 || M <= 32);
+}
+__host__ __device__ constexpr int tw_section(int M) {   // first entry of length M's section
+  int o = kTw960;
+  for (int m = 1; m < M; ++m) o += tw_own_section(m) ? m : 0;
+  return o;
+}
+constexpr int kTwN = tw_section(kTwMaxM + 1);
 static __constant__ double2 c_tw64[kTwN];
 static __constant__ float2 c_tw32[kTwN];
 
@@ -94,10 +119,20 @@ template <typename C> __device__ __forceinline__ C tw_load(int idx);
 template <> __device__ __forceinline__ double2 tw_load<double2>(int idx) { return c_tw64[idx]; }
 template <> __device__ __forceinline__ float2 tw_load<float2>(int idx) { return c_tw32[idx]; }
 
-// exp(-+ 2 pi i e / M) (INV selects +)
-template <typename C, bool INV>
-__device__ __forceinline__ C twiddle(int e, int M) {
-  C w = tw_load<C>(((e % M) * (kTwN / M)) % kTwN);
+// exp(-+ 2 pi i e / M) (INV selects +), e >= 0.  Lengths dividing 960 read
+// the shared 960-entry part (equal twiddles of different lengths, W_8^1 and
+// W_32^4, are one entry), the others their own section.
+template <typename C, bool INV, int M>
+__device__ __forceinline__ C twiddle(int e) {
+  static_assert(M >= 1 && M <= kTwMaxM && (kTw960 % M == 0 || tw_own_section(M)), "twiddle length");
+  int idx;
+  if constexpr (kTw960 % M == 0) {
+    idx = ((e % M) * (kTw960 / M)) % kTw960;
+  } else {
+    constexpr int off = tw_section(M);
+    idx = off + e % M;
+  }
+  C w = tw_load<C>(idx);
   if (INV) w.y = -w.y;
   return w;
 }
@@ -189,12 +224,19 @@ __device__ __forceinline__ void dft_small(C (&v)[R]) {
     v[2] = a2 - ib2;
     v[3] = a2 + ib2;
   } else {
+    // any other prime factor (7, 11, ..., 31: bandlimits and grids off the
+    // 2/3/5 sizes): a direct DFT, its outer loop kept rolled so that the code
+    // stays small (the outputs go through a local array)
     C o[R];
-#pragma unroll
+#pragma unroll 1
     for (int q = 0; q < R; ++q) {
       C acc = v[0];
+      int e = q;   // r q mod R
 #pragma unroll
-      for (int r = 1; r < R; ++r) acc = cfma(v[r], twiddle<C, INV>(r * q, R), acc);
+      for (int r = 1; r < R; ++r) {
+        acc = cfma(v[r], twiddle<C, INV, R>(e), acc);
+        e = e + q >= R ? e + q - R : e + q;
+      }
       o[q] = acc;
     }
 #pragma unroll
@@ -222,7 +264,7 @@ __device__ __forceinline__ void fft_stages(C (&x)[N]) {
       for (int r = 0; r < R; ++r) v[r] = x[j + r * (N / R)];
 #pragma unroll
       for (int r = 1; r < R; ++r)
-        if ((r * k) % (Ns * R) != 0) v[r] = cmul(v[r], twiddle<C, INV>(r * k, Ns * R));
+        if ((r * k) % (Ns * R) != 0) v[r] = cmul(v[r], twiddle<C, INV, Ns * R>(r * k));
       dft_small<R, INV>(v);
       const int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll

@@ -897,18 +897,15 @@ static int run_deriv(hp_plan* p, const double2* Fev, const double2* F0, double a
                      double2* acc, double bacc, cudaStream_t s, const DerivParams& prm, const void* Gx,
                      const void* fev32 = nullptr, void* out32 = nullptr) {
   switch (p->N) {
-    case 4: return run_deriv_N<4, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 6: return run_deriv_N<6, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 8: return run_deriv_N<8, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 12: return run_deriv_N<12, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 16: return run_deriv_N<16, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 20: return run_deriv_N<20, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 24: return run_deriv_N<24, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 30: return run_deriv_N<30, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 32: return run_deriv_N<32, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
-    case 40: case 48: case 60: return run_deriv_lines<T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
+#define X(n) case n: return run_deriv_N<n, T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx, fev32, out32);
+    HP_FOR_EACH_N_TO_32(X)
+#undef X
+#define X(n) case n:
+    HP_FOR_EACH_N_ABOVE_32(X)
+#undef X
+      return run_deriv_lines<T>(p, Fev, F0, a, out, acc, bacc, s, prm, Gx);
     default:
-      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24, 30 or 32)");
+      hp_set_error("omega grid size 2Bx not supported (even, 4..64)");
       return HP_ERR_UNSUPPORTED;
   }
 }
@@ -1101,17 +1098,11 @@ static int noalloc_N(hp_plan* p, const double2* Ffull, double2* dFfull, unsigned
 template <typename T>
 static int noalloc_T(hp_plan* p, const double2* F, double2* dF, unsigned char* base, const DerivParams& prm) {
   switch (p->N) {
-    case 4: return noalloc_N<4, T>(p, F, dF, base, prm);
-    case 6: return noalloc_N<6, T>(p, F, dF, base, prm);
-    case 8: return noalloc_N<8, T>(p, F, dF, base, prm);
-    case 12: return noalloc_N<12, T>(p, F, dF, base, prm);
-    case 16: return noalloc_N<16, T>(p, F, dF, base, prm);
-    case 20: return noalloc_N<20, T>(p, F, dF, base, prm);
-    case 24: return noalloc_N<24, T>(p, F, dF, base, prm);
-    case 30: return noalloc_N<30, T>(p, F, dF, base, prm);
-    case 32: return noalloc_N<32, T>(p, F, dF, base, prm);
+#define X(n) case n: return noalloc_N<n, T>(p, F, dF, base, prm);
+    HP_FOR_EACH_N_TO_32(X)
+#undef X
     default:
-      hp_set_error("omega grid size 2Bx not supported (use 4, 6, 8, 12, 16, 20, 24, 30 or 32)");
+      hp_set_error("the allocation-free derivative covers omega grids of 4..32 points per axis");
       return HP_ERR_UNSUPPORTED;
   }
 }

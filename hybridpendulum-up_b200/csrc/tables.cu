@@ -8,13 +8,18 @@
 using namespace hp;
 
 int hp::tw_fill_host(double2* t64, float2* t32) {
-  for (int k = 0; k < kTwN; ++k) {
-    // exp(-2 pi i k / 960) evaluated in long double, rounded once
-    const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / kTwN;
+  // exp(-2 pi i e / M) evaluated in long double, rounded to FP64 (and the
+  // FP64 value to FP32)
+  auto put = [&](int k, int e, int M) {
+    const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / M;
     const double c = (double)cosl(a), s = (double)sinl(a);
     t64[k] = make_double2(c, s);
     t32[k] = make_float2((float)c, (float)s);
-  }
+  };
+  for (int k = 0; k < kTw960; ++k) put(k, k, kTw960);
+  for (int M = 1; M <= kTwMaxM; ++M)
+    if (tw_own_section(M))
+      for (int e = 0; e < M; ++e) put(tw_section(M) + e, e, M);
   return 0;
 }
 

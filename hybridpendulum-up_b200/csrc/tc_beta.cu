@@ -739,7 +739,10 @@ int tc_beta_forward(hp_plan* p, const float2* Qg, const int2* pairs, int npairs,
     return HP_ERR_UNSUPPORTED;
   }
   const bool bf16 = p->beta_engine == HP_BETA_TENSOR_BF16;
-  const int KP = bf16 ? (2 * p->B + 15) / 16 * 16 : (2 * p->B + 7) / 8 * 8;
+  // nodes padded to the kernels' K: multiples of 16 (BF16) or of 8 with 56
+  // taken up to 64 (TF32); the padding rows of the operand tables are zero
+  const int k8 = (2 * p->B + 7) / 8 * 8;
+  const int KP = bf16 ? (2 * p->B + 15) / 16 * 16 : (k8 == 56 ? 64 : k8);
   int st = HP_OK;
   const char* tkey = bf16 ? "tf.dwtc16" : "tf.dwtc";
   bool have = false, have_err = false;

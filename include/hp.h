@@ -83,7 +83,12 @@ typedef struct {
 /* Plan: tables (Wigner-d, quadrature weights, Clebsch-Gordan, twiddles) are
  * built on the device in FP64.  Replaces the per-call setup of every MEX
  * (e.g. propagation/mex/sources/fftSO3R/kernel.cu:20-130) and the MATLAB table
- * builders Wigner_d.m:1-47, getu.m:132-163, clebsch_gordan.m:1-43. */
+ * builders Wigner_d.m:1-47, getu.m:132-163, clebsch_gordan.m:1-43.
+ * B: 2..32 (2B-point Euler grids); Bx: 2..32 (2Bx-point omega axes).  FFT
+ * lengths whose prime factors are 2, 3 and 5 (2B, 2Bx in 4, 6, 8, 10, 12,
+ * 16, 18, 20, 24, 30, 32, 36, 40, 48, 50, 54, 60, 64) run the fastest
+ * kernels; other lengths use a direct DFT for their larger prime factor.
+ * The derivative takes 3-D grids of up to 32 points per axis. */
 int hp_plan_create(hp_plan** plan, int B, int Bx, int ndim, int precision, int symmetry);
 int hp_plan_destroy(hp_plan* plan);
 int hp_plan_get_info(const hp_plan* plan, hp_plan_info_t* info);

@@ -29,9 +29,11 @@ def test_every_declared_symbol_is_exported(hp):
 def test_argument_validation_without_gpu(hp):
     lib = hp._lib
     h = ctypes.c_void_p()
-    assert lib.hp_plan_create(ctypes.byref(h), 7, 2, 3, 0, 0) == hp.HP_ERR_INVALID      # B not supported
+    assert lib.hp_plan_create(ctypes.byref(h), 33, 2, 3, 0, 0) == hp.HP_ERR_INVALID     # B above 32
     assert b'bandlimit' in lib.hp_last_error()
-    assert lib.hp_plan_create(ctypes.byref(h), 4, 5, 3, 0, 0) == hp.HP_ERR_INVALID      # 2Bx = 10
+    assert lib.hp_plan_create(ctypes.byref(h), 1, 2, 3, 0, 0) == hp.HP_ERR_INVALID      # B below 2
+    assert lib.hp_plan_create(ctypes.byref(h), 4, 33, 3, 0, 0) == hp.HP_ERR_INVALID     # 2Bx = 66
+    assert lib.hp_plan_create(ctypes.byref(h), 4, 1, 3, 0, 0) == hp.HP_ERR_INVALID      # 2Bx = 2
     assert lib.hp_plan_create(ctypes.byref(h), 4, 2, 4, 0, 0) == hp.HP_ERR_INVALID      # ndim
     assert lib.hp_plan_create(ctypes.byref(h), 4, 2, 3, 5, 0) == hp.HP_ERR_INVALID      # precision
     assert lib.hp_plan_create(None, 4, 2, 3, 0, 0) == hp.HP_ERR_INVALID

@@ -204,7 +204,7 @@ def test_gravity_rejects_alpha_dependent_multiplier(hp):
 
 def test_errors(hp):
     with pytest.raises(hp.HPError) as e:
-        hp.Plan(7, 2, 3)
+        hp.Plan(33, 2, 3)
     assert e.value.code == hp.HP_ERR_INVALID
     plan = hp.Plan(3, 2, 3)
     F = np.zeros(plan.F_shape, np.complex128)
