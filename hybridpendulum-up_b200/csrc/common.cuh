@@ -344,6 +344,35 @@ __device__ __forceinline__ void fft(C (&x)[N]) {
   else fft_stages<N, 1, INV>(x);
 }
 
+// 2H-point DFT over a lane pair: lanes 2t and 2t+1 of a warp (threadIdx.x of
+// a 1-D block) hold the same transform, lane h = threadIdx.x & 1 the inputs
+// x[j] = input[2j + h], j < H.  Each lane transforms its half (even or odd
+// samples), the odd half is twisted by W_2H^k, and one exchange by shuffles
+// finishes the radix-2 step: on return lane h holds output[h H + k], k < H.
+// The shuffles name the two lanes of the pair only, so pairs of one warp may
+// take different paths; both lanes of a pair must call it together.
+template <int H, bool INV, typename C>
+__device__ __forceinline__ void fft_lane_pair(C (&x)[H], int h) {
+  using T = decltype(x[0].x);
+  const unsigned pm = 3u << (threadIdx.x & 30u);
+  fft<H, INV>(x);
+#pragma unroll
+  for (int k = 1; k < H; ++k) {
+    const C t = cmul(x[k], twiddle<C, INV, 2 * H>(k));
+    x[k].x = h ? t.x : x[k].x;
+    x[k].y = h ? t.y : x[k].y;
+  }
+  // lane 0 (even half E): E + W O ; lane 1 (holding W O, receiving E): E - W O
+  const T sg = h ? (T)-1 : (T)1;
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    const T ox = __shfl_xor_sync(pm, x[k].x, 1);
+    const T oy = __shfl_xor_sync(pm, x[k].y, 1);
+    x[k].x = fma(sg, x[k].x, ox);
+    x[k].y = fma(sg, x[k].y, oy);
+  }
+}
+
 // Fourier index k (FFT order) -> signed wavenumber with the Nyquist bin zeroed
 // (the 2 pi i [0:Bx-1, 0, -Bx+1:-1] / L multiplier of the first derivative).
 __host__ __device__ __forceinline__ int kappa_first(int k, int N) {

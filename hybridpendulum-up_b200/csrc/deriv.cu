@@ -383,11 +383,16 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
   __syncthreads();
 
   // ---- S4: physical-space products, forward FFT along k2 ----
-  // item (c, j1, kind): kind 0 -> A column, kind 1 -> Y1' column
+  // item (c, j1, kind): kind 0 -> A column, kind 1 -> Y1' column.  Each item
+  // runs on a lane pair (fft_lane_pair): lane h forms the products at the rows
+  // j2 = 2j + h and ends with the wavenumbers k2 = h N/2 + k, so both stages
+  // give every thread of the block half an FFT.
+  constexpr int H = N / 2;
+  const int h = tid & 1, pr = tid >> 1, npr = nth >> 1;
   const T d3 = HAS_P3 ? tp * (T)kappa_first(k3, N) : (T)0;
   const T b1 = (T)prm.b[0], b2 = (T)prm.b[1], b3 = (T)prm.b[2];
   const T g1 = (T)prm.gyro[0], g2 = (T)prm.gyro[1], g3 = (T)prm.gyro[2];
-  for (int it = tid; it < tl.cnt * N * 2; it += nth) {
+  for (int it = pr; it < tl.cnt * N * 2; it += npr) {   // both lanes of a pair hold the same item
     const int kind = it / (tl.cnt * N);
     const int c = (it / N) % tl.cnt;
     const int j1 = it % N;
@@ -399,11 +404,12 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
     const int n = tl.n0 + c, l = tl.l;
     const T lie = (T)prm.lie;
     const T ap = lie * sqrt((T)((l - n) * (l + n + 1))), am = lie * sqrt((T)((l + n) * (l - n + 1)));
-    C x[N];
+    C x[H];
     if (kind == 0) {
       // Y0 = a+ F~+ (0.5i x1 - 0.5 x2) + a- F~- (0.5i x1 + 0.5 x2) - g3 D3 x1 x2 F~ + (i n + b3 D3) P~
 #pragma unroll
-      for (int j2 = 0; j2 < N; ++j2) {
+      for (int j = 0; j < H; ++j) {
+        const int j2 = 2 * j + h;
         const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
         const int o = j2 * (N + 1) + j1;
         const C vp = fp[o], vm = fm[o];
@@ -415,76 +421,81 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
         if (HAS_P3) {
           const C v0 = f0[o], pv = pp[o];
           // - g3 (i d3) x1 x2 v0
-          const T s = g3 * d3 * x1 * x2;
-          y.x += s * v0.y;
-          y.y -= s * v0.x;
+          const T sg = g3 * d3 * x1 * x2;
+          y.x += sg * v0.y;
+          y.y -= sg * v0.x;
           // (i n + b3 i d3) pv = i (n + b3 d3) pv
           const T q = lie * (T)n + b3 * d3;
           y.x -= q * pv.y;
           y.y += q * pv.x;
         }
-        x[j2] = y;
+        x[j] = y;
       }
-      fft<N, false>(x);
+      fft_lane_pair<H, false>(x, h);
 #pragma unroll
-      for (int j = 0; j < N; ++j) sA[c * PS + j * (N + 1) + j1] = x[j];
+      for (int k = 0; k < H; ++k) sA[c * PS + (h * H + k) * (N + 1) + j1] = x[k];
       // Y2 = b2 x2 F~ - g2 x1 P~  -> FFT_2 -> times D_2 = i d2(k2), added to A
 #pragma unroll
-      for (int j2 = 0; j2 < N; ++j2) {
+      for (int j = 0; j < H; ++j) {
+        const int j2 = 2 * j + h;
         const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
         const int o = j2 * (N + 1) + j1;
         C y = (b2 * x2) * f0[o];
         if (HAS_P3) y = y - (g2 * x1) * pp[o];
-        x[j2] = y;
+        x[j] = y;
       }
-      fft<N, false>(x);
+      fft_lane_pair<H, false>(x, h);
 #pragma unroll
-      for (int k2 = 0; k2 < N; ++k2) {
+      for (int k = 0; k < H; ++k) {
+        const int k2 = h * H + k;
         const T dk = tp * (T)kappa_first(k2, N);
         C* dst = sA + c * PS + k2 * (N + 1) + j1;
         C v = *dst;
-        v.x -= dk * x[k2].y;
-        v.y += dk * x[k2].x;
+        v.x -= dk * x[k].y;
+        v.y += dk * x[k].x;
         *dst = v;
       }
     } else {
       // Y1 = b1 x1 F~ - g1 x2 P~
 #pragma unroll
-      for (int j2 = 0; j2 < N; ++j2) {
+      for (int j = 0; j < H; ++j) {
+        const int j2 = 2 * j + h;
         const T x2 = -Ll / 2 + Ll * (T)j2 / (T)N;
         const int o = j2 * (N + 1) + j1;
         C y = (b1 * x1) * f0[o];
         if (HAS_P3) y = y - (g1 * x2) * pp[o];
-        x[j2] = y;
+        x[j] = y;
       }
-      fft<N, false>(x);
+      fft_lane_pair<H, false>(x, h);
 #pragma unroll
-      for (int j = 0; j < N; ++j) sY[c * PS + j * (N + 1) + j1] = x[j];
+      for (int k = 0; k < H; ++k) sY[c * PS + (h * H + k) * (N + 1) + j1] = x[k];
     }
   }
   __syncthreads();
 
-  // ---- S5: forward FFT along k1; Y1' gets D_1 ----
-  for (int it = tid; it < tl.cnt * N * 2; it += nth) {
+  // ---- S5: forward FFT along k1 (lane pairs, in place); Y1' gets D_1 ----
+  // The lanes of a pair read all of the row before their first exchange and
+  // write it after, so the in-place update is safe.
+  for (int it = pr; it < tl.cnt * N * 2; it += npr) {
     const int kind = it / (tl.cnt * N);
     const int c = (it / N) % tl.cnt;
     const int k2 = it % N;
     C* pl = (kind == 0 ? sA : sY) + c * PS + k2 * (N + 1);
-    C x[N];
+    C x[H];
 #pragma unroll
-    for (int j = 0; j < N; ++j) x[j] = pl[j];
-    fft<N, false>(x);
+    for (int j = 0; j < H; ++j) x[j] = pl[2 * j + h];
+    fft_lane_pair<H, false>(x, h);
     if (kind == 0) {
 #pragma unroll
-      for (int j = 0; j < N; ++j) pl[j] = x[j];
+      for (int k = 0; k < H; ++k) pl[h * H + k] = x[k];
     } else {
 #pragma unroll
-      for (int k1 = 0; k1 < N; ++k1) {
-        const T dk = tp * (T)kappa_first(k1, N);
+      for (int k = 0; k < H; ++k) {
+        const T dk = tp * (T)kappa_first(h * H + k, N);
         C v;
-        v.x = -dk * x[k1].y;
-        v.y = dk * x[k1].x;
-        pl[k1] = v;
+        v.x = -dk * x[k].y;
+        v.y = dk * x[k].x;
+        pl[h * H + k] = v;
       }
     }
   }
