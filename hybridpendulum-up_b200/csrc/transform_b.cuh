@@ -81,6 +81,30 @@ __device__ __forceinline__ float4 unrotate4(float4 v, int rot) {
 // computes the NB x PT tile of one (m, n) pair, so each coefficient load (PT
 // consecutive omega points, one vector load) feeds NB x PT complex FMAs and
 // each d value PT of them.
+// Two staging runs of N floats (the real and the imaginary parts of x), both
+// starting LEAD floats (0 or 2) before a 16-byte boundary: an 8-byte store
+// for the lead, 16-byte stores, an 8-byte store for an even remainder.
+template <int N, int LEAD>
+__device__ __forceinline__ void stage_run(float* st, float* st2, const float2 (&x)[N]) {
+  static_assert(N % 2 == 0 && (LEAD == 0 || LEAD == 2), "even runs, 8-byte aligned");
+  if constexpr (LEAD == 2) {
+    *reinterpret_cast<float2*>(st) = make_float2(x[0].x, x[1].x);
+    *reinterpret_cast<float2*>(st2) = make_float2(x[0].y, x[1].y);
+  }
+  constexpr int n4 = (N - LEAD) / 4;
+#pragma unroll
+  for (int i = 0; i < n4; ++i) {
+    const int a = LEAD + 4 * i;
+    *reinterpret_cast<float4*>(st + a) = make_float4(x[a].x, x[a + 1].x, x[a + 2].x, x[a + 3].x);
+    *reinterpret_cast<float4*>(st2 + a) = make_float4(x[a].y, x[a + 1].y, x[a + 2].y, x[a + 3].y);
+  }
+  constexpr int a = LEAD + 4 * n4;
+  if constexpr (a < N) {
+    *reinterpret_cast<float2*>(st + a) = make_float2(x[a].x, x[a + 1].x);
+    *reinterpret_cast<float2*>(st2 + a) = make_float2(x[a].y, x[a + 1].y);
+  }
+}
+
 template <int B, typename T, int NB, int P, bool CPLX, bool GD, int PT = 1>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
     k_synth(RowLayout L, const c2<T>* __restrict__ Fp, const T* __restrict__ wig, const int2* __restrict__ pairs,
@@ -260,6 +284,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 1 : 2)
         C* st = sG + ((p * NB2 + c) * NB + bb) * NB2;
 #pragma unroll
         for (int a = 0; a < NB2; ++a) st[a] = x[a];
+      } else if constexpr (BULK) {
+        // runs start on 4-float boundaries (RS is a multiple of 4): 16-byte
+        // stores, after one 8-byte store where bb * 2B is 2 mod 4 (2B even)
+        float* st = reinterpret_cast<float*>(sG) + (p * NB2 + c) * RS + bb * NB2;
+        float* st2 = reinterpret_cast<float*>(sG) + (p * NB2 + c + B) * RS + bb * NB2;
+        if (((bb * NB2) & 3) == 0) stage_run<NB2, 0>(st, st2, x);
+        else stage_run<NB2, 2>(st, st2, x);
       } else {
         T* st = reinterpret_cast<T*>(sG) + (p * NB2 + c) * RS;
         T* st2 = reinterpret_cast<T*>(sG) + (p * NB2 + c + B) * RS;
