@@ -48,11 +48,12 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--fp64-steps', type=int, default=None)
-    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform', 'hybrid', 'forward'],
+    ap.add_argument('--workload', default='step', choices=['step', 'batch', 'transform', 'hybrid', 'forward', 'adjoint'],
                     help='step: the headline FP step; batch: uneven-bandlimit batch of densities; '
                          'transform: B=32 round-trip precision stress; hybrid: the loop of '
                          'pendulum_reduced_hybrid.m at its own sizes (B=30, 60x60 omega); '
-                         'forward: one FP32 forward transform on a 2-D omega grid (--B, --Bx, --beta-engine)')
+                         'forward: one FP32 forward transform on a 2-D omega grid (--B, --Bx, --beta-engine); '
+                         'adjoint: the gradient of a terminal loss through 50 Euler steps at B=12, 24^3')
     ap.add_argument('--members', type=int, default=64)
     ap.add_argument('--persistent', action='store_true',
                     help='batch workload: plane passes of the plain members in one persistent launch per round')
@@ -293,6 +294,8 @@ def main():
         return bench_hybrid(args, rank, local)
     if args.workload == 'forward':
         return bench_forward(args, rank, local)
+    if args.workload == 'adjoint':
+        return bench_adjoint(args, rank, local)
     if args.impl == 'reference':
         if rank != 0:
             return 0
@@ -756,6 +759,67 @@ def bench_forward(args, rank, local):
             'config': {'workload': 'forward transform', 'B': B, 'omega_grid': f'{2 * Bx}x{2 * Bx}',
                        'beta_engine': args.beta_engine},
             'kernel_ms_per_launch': fam, 'tc_errors': plan.tc_errors(), 'launch_shapes': plan.get_tune()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def bench_adjoint(args, rank, local):
+    """The differentiation workload: gradients of a terminal loss
+    <lamT, F_T> with respect to the initial coefficients and the damping,
+    gyroscopic, noise and gravity parameters through 50 Euler steps
+    (dt = 1e-3) at B=12 on a 24^3 omega grid, FP64 plan, checkpoints every
+    10 steps (hp_pendulum_adjoint: forward sweep keeping checkpoints, then
+    the reverse sweep recomputing each segment), device-resident.  Timed with
+    CUDA events beside the plain 50-step forward propagation it
+    differentiates.  Prints one JSON line (not the headline)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    hp = importlib.import_module('hybridpendulum-up_b200')
+    B, Bx, nsteps, ckpt = 12, 12, 50, 10
+    inp = model_inputs(hp, B, Bx, seed=replica_seed(rank))
+    L, dt = PARAMS['L'], PARAMS['dt']
+    stream = torch.cuda.current_stream(dev)
+    plan = hp.Plan(B, Bx, 3, hp.HP_FP64, hp.HP_REAL)
+    plan.set_stream(stream.cuda_stream)
+    plan.set_model(L, inp['b'], inp['G'], inp['MR'], inp['gyro'])
+    f0 = initial_density_dev(torch, inp, B, Bx, L, dev)
+    n = int(np.prod(plan.F_shape))
+    F0 = torch.zeros(n, dtype=torch.complex128, device=dev)
+    plan.forward(f0, out=F0)
+    del f0
+    g = torch.Generator(device=dev).manual_seed(5 + rank)
+    lamT = torch.randn(n, dtype=torch.complex128, device=dev, generator=g)
+    st = hp.State(plan)
+
+    def forward_only():
+        st.load(F0)
+        st.step(dt, 'euler', nsteps)
+
+    def timed(fn, K, W):
+        for _ in range(W):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / K
+
+    K, W = max(1, min(args.steps, 5)), max(args.warmup, 1)
+    ms_adj = timed(lambda: plan.adjoint(F0, lamT, nsteps, dt, ckpt), K, W)
+    ms_fwd = timed(forward_only, K, W)
+    lam0, grads = plan.adjoint(F0, lamT, nsteps, dt, ckpt)
+    line = {'metric': 'gradient of a terminal loss through 50 Euler steps, B=12, omega 24^3, FP64',
+            'value': round(ms_adj, 3), 'unit': 'ms per gradient', 'higher_is_better': False, 'n_gpus': 1,
+            'steps': K, 'warmup': W, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': 'adjoint (config 4)', 'B': B, 'omega_grid': '24^3', 'nsteps': nsteps,
+                       'checkpoint_every': ckpt, 'gradients': ['F0', 'b', 'G', 'gyro', 'gscale']},
+            'forward_50_steps_ms': round(ms_fwd, 3), 'reverse_over_forward': round(ms_adj / ms_fwd, 2),
+            'grad_b': [float(x) for x in grads['b']]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

@@ -97,6 +97,50 @@ __global__ void __launch_bounds__(128) k_axis_md(RowLayout L, const double2* __r
   }
 }
 
+// out (=, or += with acc) coef * D_daxis (M_axis in): one thread per line of N
+// points along `axis`; M_axis multiplies by x_axis on the omega grid
+// (inverse FFT, times x, FFT), D_daxis by 2 pi i kappa / L along axis daxis
+// (any axis, applied per point after M; daxis < 0: none).
+template <int N>
+__global__ void __launch_bounds__(128) k_line_dm(RowLayout L, const double2* __restrict__ in,
+                                                 double2* __restrict__ out, int axis, int daxis, double coef,
+                                                 double Llen, int acc) {
+  const long long nlines = L.nx / N;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= L.nrows * nlines) return;
+  const long long row = t / nlines, q = t % nlines;
+  long long stride = 1, dstride = 1;
+  for (int a = 0; a < axis; ++a) stride *= N;
+  for (int a = 0; a < daxis; ++a) dstride *= N;
+  const long long lo = q % stride, hi = q / stride;
+  const long long w0 = hi * stride * N + lo;   // omega index of the line's first point
+  const long long base = row * L.nx + w0;
+  const double tp = 2.0 * M_PI / Llen;
+  double2 x[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) x[j] = in[base + j * stride];
+  fft<N, true>(x);
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const double xc = (-Llen / 2 + Llen * j / N) / N;
+    x[j] = xc * x[j];
+  }
+  fft<N, false>(x);
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    double2 v = x[j];
+    if (daxis >= 0) {   // i dk v
+      const long long w = w0 + j * stride;
+      const double dk = tp * kappa_first((int)((w / dstride) % N), N);
+      v = make_double2(-dk * v.y, dk * v.x);
+    }
+    double2 o = acc ? out[base + j * stride] : make_double2(0.0, 0.0);
+    o.x += coef * v.x;
+    o.y += coef * v.y;
+    out[base + j * stride] = o;
+  }
+}
+
 __device__ __forceinline__ double row_weight(const RowLayout& L, long long row, int half) {
   return (half && L.rows[row].y > 0) ? 2.0 : 1.0;
 }
@@ -195,6 +239,29 @@ int axis_md_launch(hp_plan* p, const double2* in, double2* out, int axis, double
   return HP_OK;
 }
 
+template <int N>
+int line_dm_launch(hp_plan* p, const double2* in, double2* out, int axis, int daxis, double coef, int acc,
+                   cudaStream_t s) {
+  const long long nl = p->nrows * (p->nx / N);
+  ProfScope _ps(p, "adj.axis", s);
+  k_line_dm<N><<<(unsigned)((nl + 127) / 128), 128, 0, s>>>(p->layout(), in, out, axis, daxis, coef, p->model.L, acc);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
+// out = coef D_daxis M_axis in (acc: out += ...)
+int line_dm(hp_plan* p, const double2* in, double2* out, int axis, int daxis, double coef, int acc,
+            cudaStream_t s) {
+  switch (p->N) {
+#define X(n) case n: return line_dm_launch<n>(p, in, out, axis, daxis, coef, acc, s);
+    HP_FOR_EACH_N(X)
+#undef X
+    default:
+      hp_set_error("omega grid size 2Bx not supported (even, 4..64)");
+      return HP_ERR_UNSUPPORTED;
+  }
+}
+
 int axis_md(hp_plan* p, const double2* in, double2* out, int axis, double coef, cudaStream_t s) {
   switch (p->N) {
 #define X(n) case n: return axis_md_launch<n>(p, in, out, axis, coef, s);
@@ -240,7 +307,13 @@ int adjoint_apply(hp_plan* p, const double2* lam, double2* out, double a, int ad
 // ((0,0),(0,1),(0,2),(1,1),(1,2),(2,2)).
 constexpr int kSlots = 15;
 
-// acc += dt * Re<lam, dA/dtheta F> for every parameter theta.
+// acc += dt * Re<lam, dA/dtheta F> for every parameter theta.  The terms of
+// the derivative are linear in their parameters, so dA/dtheta F is the term
+// itself with unit coefficient, each formed by the passes it needs alone:
+//   damping   dA/db_i F    =  D_i M_i F            (one line pass)
+//   gyroscope dA/dgyro_i F = -D_i M_j M_k F        (two line passes; j, k the other axes)
+//   gravity   dA/dgs_i F   =  the gravity pass with component i alone
+// (the forms of the plane pass's Y0, Y1, Y2 products and the axis-3 pass).
 int grad_terms(hp_plan* p, const double2* lam, const double2* F, double dt, double* acc, cudaStream_t s) {
   const DerivParams base = hp_model_params(p);
   int st = HP_OK;
@@ -248,35 +321,34 @@ int grad_terms(hp_plan* p, const double2* lam, const double2* F, double dt, doub
   double2* y = (double2*)p->ws_get("adj.y", ib, &st);
   if (st) return st;
   const int half = p->symmetry == HP_REAL;
-  auto zero = [&]() {
-    DerivParams z = base;
-    for (int i = 0; i < 3; ++i) { z.b[i] = 0; z.gyro[i] = 0; z.gs[i] = 0; }
-    for (int i = 0; i < 9; ++i) z.G[i] = 0;
-    z.lie = 0;
-    return z;
-  };
-  auto term = [&](const DerivParams& z, int slot) -> int {
-    ADJ_CHECK(hp_derivative_eval_prm(p, z, F, nullptr, 1.0, y, nullptr, 0.0, s));
+  auto dot = [&](int slot) -> int {
     ProfScope _ps(p, "adj.dot", s);
     k_dot<<<kDotBlocks, kDotThreads, 0, s>>>(p->layout(), lam, y, acc, slot, dt, half);
     HP_CUDA_TRY(cudaGetLastError());
     return HP_OK;
   };
   for (int i = 0; i < p->ndim; ++i) {
-    DerivParams z = zero();
-    z.b[i] = 1.0;
-    ADJ_CHECK(term(z, i));
+    ADJ_CHECK(line_dm(p, F, y, i, i, 1.0, 0, s));
+    ADJ_CHECK(dot(i));
   }
-  if (p->ndim == 3)
+  if (p->ndim == 3) {
+    double2* t = (double2*)p->ws_get("adj.t", ib, &st);
+    if (st) return st;
     for (int i = 0; i < 3; ++i) {
-      DerivParams z = zero();
-      z.gyro[i] = 1.0;
-      ADJ_CHECK(term(z, 3 + i));
+      const int j = (i + 1) % 3, k = (i + 2) % 3;
+      ADJ_CHECK(line_dm(p, F, t, j, -1, 1.0, 0, s));
+      ADJ_CHECK(line_dm(p, t, y, k, i, -1.0, 0, s));
+      ADJ_CHECK(dot(3 + i));
     }
+  }
   for (int i = 0; i < p->ndim; ++i) {
-    DerivParams z = zero();
+    DerivParams z = base;
+    for (int a = 0; a < 3; ++a) { z.b[a] = 0; z.gyro[a] = 0; z.gs[a] = 0; }
+    for (int a = 0; a < 9; ++a) z.G[a] = 0;
+    z.lie = 0;
     z.gs[i] = 1.0;
-    ADJ_CHECK(term(z, 6 + i));
+    ADJ_CHECK(hp_gravity_noise_eval64(p, z, F, y, s));
+    ADJ_CHECK(dot(6 + i));
   }
   ProfScope _ps(p, "adj.dot", s);
   k_dot_noise<<<kDotBlocks, kDotThreads, 0, s>>>(p->layout(), lam, F, acc, 9, dt, half, p->model.L);

@@ -1005,6 +1005,11 @@ int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Fe
 // out = F0 + a * dF(Feval); if acc: acc += bacc * dF(Feval).  F0 may be null (zero).
 // With a density-gravity model (hp_pendulum_propagate_den), fgrid is the grid
 // density of Feval when the caller has it (else it is recomputed from Feval).
+int hp_gravity_noise_eval64(hp_plan* p, const DerivParams& prm, const double2* F, double2* out, cudaStream_t s) {
+  if (tw_init() != 0) { hp_set_error("twiddle table upload failed"); return HP_ERR_CUDA; }
+  return launch_local<double, double>(p, F, out, nullptr, prm, s);
+}
+
 int hp_derivative_eval(hp_plan* p, const double2* Fev, const double2* F0, double a, double2* out,
                        double2* acc, double bacc, cudaStream_t s, const void* fgrid, const void* fev32,
                        void* out32) {

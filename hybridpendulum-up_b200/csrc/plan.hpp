@@ -199,6 +199,10 @@ DerivParams hp_model_params(const hp_plan* p);
 int hp_derivative_eval_prm(hp_plan* p, const DerivParams& prm, const double2* Feval, const double2* F0,
                            double a, double2* out, double2* acc, double bacc, cudaStream_t s,
                            const void* fgrid = nullptr, const void* fev32 = nullptr, void* out32 = nullptr);
+// The gravity and noise terms of the derivative alone (the pointwise-in-omega
+// pass), in FP64 whatever the plan's precision: out = noise F + gravity F
+// ([row][omega] layout, FP64 in and out).
+int hp_gravity_noise_eval64(hp_plan* p, const DerivParams& prm, const double2* F, double2* out, cudaStream_t s);
 int hp_derivative_eval(hp_plan* p, const double2* Feval, const double2* F0, double a,
                        double2* out, double2* acc, double bacc, cudaStream_t s,
                        const void* fgrid = nullptr, const void* fev32 = nullptr, void* out32 = nullptr);
