@@ -812,13 +812,18 @@ def bench_adjoint(args, rank, local):
     K, W = max(1, min(args.steps, 5)), max(args.warmup, 1)
     ms_adj = timed(lambda: plan.adjoint(F0, lamT, nsteps, dt, ckpt), K, W)
     ms_fwd = timed(forward_only, K, W)
+    plan.profile(True)
     lam0, grads = plan.adjoint(F0, lamT, nsteps, dt, ckpt)
+    torch.cuda.synchronize()
+    fam = {k: round(v[0], 2) for k, v in plan.profile_read().items()}   # ms per gradient by kernel family
+    plan.profile(False)
     line = {'metric': 'gradient of a terminal loss through 50 Euler steps, B=12, omega 24^3, FP64',
             'value': round(ms_adj, 3), 'unit': 'ms per gradient', 'higher_is_better': False, 'n_gpus': 1,
             'steps': K, 'warmup': W, 'dtype': 'f64', 'data': 'synthetic',
             'config': {'workload': 'adjoint (config 4)', 'B': B, 'omega_grid': '24^3', 'nsteps': nsteps,
                        'checkpoint_every': ckpt, 'gradients': ['F0', 'b', 'G', 'gyro', 'gscale']},
             'forward_50_steps_ms': round(ms_fwd, 3), 'reverse_over_forward': round(ms_adj / ms_fwd, 2),
+            'kernel_ms_per_gradient': fam,
             'grad_b': [float(x) for x in grads['b']]}
     if rank == 0:
         print(json.dumps(line), flush=True)
