@@ -356,6 +356,23 @@ __device__ __forceinline__ void plane_body(const RowLayout& L, const PlaneTile t
   }
   __syncthreads();
 
+  // The update stage's loads (G, F0, acc) depend on nothing computed here:
+  // their 128-byte lines are prefetched into L2 now and land during the FFT
+  // stages (row offsets from s_rb, set before the barrier above).
+  {
+    const int tot = tl.cnt * N * N;
+    constexpr int EG = 128 / (int)sizeof(C);   // elements of G per line
+    for (int e = tid * EG; e < tot; e += nth * EG) {
+      const long long gi = s_rb[e / (N * N)] + e % (N * N);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(Gl + gi));
+    }
+    for (int e = tid * 8; e < tot; e += nth * 8) {   // FP64: 8 elements per line
+      const long long gi = s_rb[e / (N * N)] + e % (N * N);
+      if (F0) asm volatile("prefetch.global.L2 [%0];" ::"l"(F0 + gi));
+      if (acc) asm volatile("prefetch.global.L2 [%0];" ::"l"(acc + gi));
+    }
+  }
+
   // ---- S2/S3: inverse FFT along k1 (rows) then k2 (columns) of all loaded planes ----
   const int nLoaded = nF + (HAS_P3 ? tl.cnt : 0);
   auto plane_ptr = [&](int s) -> C* { return s < nF ? sF + s * PS : sP + (s - nF) * PS; };
