@@ -149,6 +149,15 @@ __global__ void __launch_bounds__(256) k_local(RowLayout L, const c2<TIN>* __res
       }
     }
     __syncthreads();
+    if (ch + 1 < ch1) {   // the next chunk's rows into L2 while this one computes
+      constexpr int EPL = 128 / (int)sizeof(c2<TIN>);           // elements per 128-byte line
+      constexpr int LPR = (W + EPL - 1) / EPL;                   // lines per row segment
+      const long long w1 = w0 + W;
+      for (int e = tid; e < R * LPR; e += nth) {
+        const long long ww = w1 + (long long)(e % LPR) * EPL;
+        if (ww < L.nx) asm volatile("prefetch.global.L2 [%0];" ::"l"(F + (size_t)(r0 + e / LPR) * L.nx + ww));
+      }
+    }
     const long long wg = w0 + w;
     if (wg >= L.nx) continue;
     T d1[NDIM], dd[NDIM];
