@@ -449,10 +449,15 @@ def main():
             Fh, Fn = Fn, Fh
         barrier()
         dt_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
-        bi = 2 * Fh.numel() * 16
+        # two F inputs per step: read in place from the pinned buffers (only the
+        # entries the plan keeps cross the bus) or copied whole
+        in_place = hp.host_read_in_place(Fh) and hp.host_read_in_place(Fn)
+        bi = 2 * (pmix.nrows * pmix.nx if in_place else Fh.numel()) * 16
         bo = Fh.numel() * 16 + fh.numel() * 8
         e2e = {'value': whole_job_rate(world, args.e2e_steps, dt_e2e * 1e3), 'unit': 'steps/s',
                'h2d_bytes_per_step': bi, 'd2h_bytes_per_step': bo,
+               'h2d': ('kept entries read in place from the pinned MATLAB-layout F buffers (full buffers: '
+                       f'{2 * Fh.numel() * 16} bytes)') if in_place else 'full MATLAB-layout F buffers copied',
                'api': 'hp_pendulum_propagate + hp_fftSO3R_backward, host (pinned) MATLAB-layout buffers'}
 
     cpu = None

@@ -167,6 +167,7 @@ def _load():
         'hp_tune_cache_save': [ctypes.c_char_p],
         'hp_tune_cache_load': [ctypes.c_char_p],
         'hp_batch_set_persistent': [vp, ip],
+        'hp_host_read_in_place': [vp, ctypes.c_longlong, ctypes.POINTER(ip)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -204,6 +205,22 @@ def _ptr(a, dtype):
             raise TypeError(f'expected a contiguous {tdt} tensor')
         return a.data_ptr(), (HP_DEVICE if a.is_cuda else HP_HOST)
     raise TypeError(f'unsupported array type {type(a)}')
+
+
+def host_read_in_place(a) -> bool:
+    """True when the library reads the host array `a` (an F input) in place:
+    page-locked memory mapped into the device address space, such as a torch
+    ``pin_memory`` tensor; only the entries the plan keeps then cross the bus.
+    False when it is copied whole to the device first (e.g. a numpy array)."""
+    if isinstance(a, np.ndarray):
+        p, nb = a.ctypes.data, a.nbytes
+    else:
+        if a.is_cuda:
+            raise ValueError('expected a host array')
+        p, nb = a.data_ptr(), a.numel() * a.element_size()
+    r = ctypes.c_int()
+    _check(_lib.hp_host_read_in_place(ctypes.c_void_p(p), nb, ctypes.byref(r)))
+    return bool(r.value)
 
 
 # ------------------------------------------------------------------- plan ----

@@ -226,7 +226,7 @@ extern "C" int hp_plan_create(hp_plan** out, int B, int Bx, int ndim, int precis
 
 extern "C" int hp_plan_destroy(hp_plan* p) {
   if (!p) return HP_OK;
-  hp_dev_free(p->rows); hp_dev_free(p->seg); hp_dev_free(p->wig64); hp_dev_free(p->wig32); hp_dev_free(p->wfull);
+  hp_dev_free(p->rows); hp_dev_free(p->seg); hp_dev_free(p->fgather); hp_dev_free(p->wig64); hp_dev_free(p->wig32); hp_dev_free(p->wfull);
   hp_dev_free(p->qw); hp_dev_free(p->cg1); hp_dev_free(p->tap_wr); hp_dev_free(p->tap_wr32);
   p->prof_on = false;
   prof_collect(p);
@@ -273,6 +273,42 @@ static int finish_out(hp_plan* p, void* host, const void* dev, size_t bytes, int
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   return HP_OK;
 }
+// Device address of a 16-byte aligned host buffer that is page-locked and
+// mapped into the current device's address space at its first and its last
+// byte, contiguously; null otherwise (pageable memory, a range that leaves the
+// mapping, or an alignment the kernel's 16-byte loads cannot take).
+static const void* mapped_host(const void* h, size_t bytes) {
+  if (!h || bytes == 0 || (reinterpret_cast<uintptr_t>(h) & 15u)) return nullptr;
+  cudaPointerAttributes a{}, b{};
+  if (cudaPointerGetAttributes(&a, h) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  const char* last = static_cast<const char*>(h) + (bytes - 1);
+  if (cudaPointerGetAttributes(&b, last) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+  if (b.type != cudaMemoryTypeHost || !b.devicePointer) return nullptr;
+  if (static_cast<const char*>(b.devicePointer) - static_cast<const char*>(a.devicePointer) != (ptrdiff_t)(bytes - 1))
+    return nullptr;
+  return a.devicePointer;
+}
+
+extern "C" int hp_host_read_in_place(const void* ptr, long long bytes, int* in_place) {
+  if (!ptr || !in_place || bytes <= 0) { hp_set_error("null argument or empty range"); return HP_ERR_INVALID; }
+  *in_place = mapped_host(ptr, (size_t)bytes) ? 1 : 0;
+  return HP_OK;
+}
+
+// F in the full layout (host or device) -> [row][omega] rows in Fi.  A mapped
+// host buffer is read in place, only its kept entries; another host buffer is
+// copied whole into the workspace and converted there.
+static int load_full(hp_plan* p, const double* F, int mem, double2* Fi) {
+  const size_t fb = 16 * (size_t)p->n_full();
+  if (mem == HP_HOST)
+    if (const void* m = mapped_host(F, fb)) return hp_full_gather(p, static_cast<const double2*>(m), Fi, p->stream);
+  int st = HP_OK;
+  const double2* d = (const double2*)stage_in(p, "api.Fin", F, fb, mem, &st);
+  if (st) return st;
+  return hp_full_to_internal(p, d, Fi, p->stream);
+}
+
 static int check_mem(int mem) {
   if (mem != HP_DEVICE && mem != HP_HOST) { hp_set_error("mem must be HP_DEVICE or HP_HOST"); return HP_ERR_INVALID; }
   return HP_OK;
@@ -483,11 +519,9 @@ extern "C" int hp_fftSO3R_backward(hp_plan* p, const double* F, double* f, int m
   int st = HP_OK;
   const bool cplx = p->symmetry == HP_COMPLEX;
   const long long ng = p->n_grid() * (cplx ? 2 : 1);
-  const double2* dF = (const double2*)stage_in(p, "api.Fin", F, 16 * (size_t)p->n_full(), mem, &st);
-  if (st) return st;
   double2* Fi = (double2*)p->ws_get("api.Fint", 16 * (size_t)p->nrows * p->nx, &st);
   if (st) return st;
-  HP_CHECK(hp_full_to_internal(p, dF, Fi, p->stream));
+  HP_CHECK(load_full(p, F, mem, Fi));
   double* df = (double*)stage_out(p, "api.fout", f, sizeof(double) * ng, mem, &st);
   if (st) return st;
   if (p->precision == HP_MIXED) {
@@ -557,14 +591,12 @@ extern "C" int hp_pendulum_propagate(hp_plan* p, const double* Fold, double* Fne
   if (!std::isfinite(dt)) { hp_set_error("dt must be finite"); return HP_ERR_INVALID; }
   int st = HP_OK;
   const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
-  const double2* dF = (const double2*)stage_in(p, "api.Fin", Fold, fb, mem, &st);
-  if (st) return st;
   double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
   double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
   double2* b2 = (method == HP_EULER) ? nullptr : (double2*)p->ws_get("api.S2", ib, &st); if (st) return st;
   double2* ac = (method == HP_RK2 || method == HP_RK4) ? (double2*)p->ws_get("api.S3", ib, &st) : nullptr;
   if (st) return st;
-  HP_CHECK(hp_full_to_internal(p, dF, b0, p->stream));
+  HP_CHECK(load_full(p, Fold, mem, b0));
   double2 *F = b0, *F2 = b1, *F3 = b2;
   HP_CHECK(integrate_internal(p, &F, &F2, &F3, ac, dt, method));
   double2* dOut = (double2*)stage_out(p, "api.Fout", Fnew, fb, mem, &st);
@@ -605,14 +637,12 @@ extern "C" int hp_pendulum_propagate_den(hp_plan* p, const double* Fold, const d
     }
   }
   const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
-  const double2* dF = (const double2*)stage_in(p, "api.Fin", Fold, fb, mem, &st);
-  if (st) return st;
   double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
   double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
   double2* b2 = (method == HP_EULER) ? nullptr : (double2*)p->ws_get("api.S2", ib, &st); if (st) return st;
   double2* ac = (method == HP_RK2 || method == HP_RK4) ? (double2*)p->ws_get("api.S3", ib, &st) : nullptr;
   if (st) return st;
-  HP_CHECK(hp_full_to_internal(p, dF, b0, p->stream));
+  HP_CHECK(load_full(p, Fold, mem, b0));
   double2 *F = b0, *F2 = b1, *F3 = b2;
   HP_CHECK(integrate_internal(p, &F, &F2, &F3, ac, dt, method, fg));
   double2* dOut = (double2*)stage_out(p, "api.Fout", Fnew, fb, mem, &st);
@@ -629,11 +659,9 @@ extern "C" int hp_pendulum_derivative(hp_plan* p, const double* F, double* dF, i
   if (!p->has_model) { hp_set_error("no model: call hp_plan_set_model first"); return HP_ERR_NO_MODEL; }
   int st = HP_OK;
   const size_t fb = 16 * (size_t)p->n_full(), ib = 16 * (size_t)p->nrows * p->nx;
-  const double2* dIn = (const double2*)stage_in(p, "api.Fin", F, fb, mem, &st);
-  if (st) return st;
   double2* b0 = (double2*)p->ws_get("api.S0", ib, &st); if (st) return st;
   double2* b1 = (double2*)p->ws_get("api.S1", ib, &st); if (st) return st;
-  HP_CHECK(hp_full_to_internal(p, dIn, b0, p->stream));
+  HP_CHECK(load_full(p, F, mem, b0));
   HP_CHECK(hp_derivative_eval(p, b0, nullptr, 1.0, b1, nullptr, 0.0, p->stream));
   double2* dOut = (double2*)stage_out(p, "api.Fout", dF, fb, mem, &st);
   if (st) return st;
@@ -692,10 +720,7 @@ extern "C" int hp_state_load(hp_state* s, const double* F, int mem) {
   if (!s || !F) { hp_set_error("null argument"); return HP_ERR_INVALID; }
   HP_CHECK(check_mem(mem));
   hp_plan* p = s->plan;
-  int st = HP_OK;
-  const double2* d = (const double2*)stage_in(p, "api.Fin", F, 16 * (size_t)p->n_full(), mem, &st);
-  if (st) return st;
-  HP_CHECK(hp_full_to_internal(p, d, s->F, p->stream));
+  HP_CHECK(load_full(p, F, mem, s->F));
   HP_CUDA_TRY(cudaStreamSynchronize(p->stream));
   s->fg_valid = false;
   s->f32_valid = false;

@@ -47,6 +47,9 @@ struct hp_plan {
   // device tables
   char4* rows = nullptr;
   int* seg = nullptr;
+  // the kept entries in full-layout order (m fastest, then n, then l):
+  // (full index within one omega slice, row)
+  int2* fgather = nullptr;
   double* wig64 = nullptr;   // [b][row] d^l_mn(beta_b)
   float* wig32 = nullptr;
   double* wfull = nullptr;   // d(2lmax+1,2lmax+1,lmax+1,2B) in the MATLAB layout
@@ -151,6 +154,9 @@ int hp_twiddles_init();
 int hp_build_gravity_taps(hp_plan* p);
 int hp_full_to_internal(hp_plan* p, const double2* Ffull, double2* Fint, cudaStream_t s);
 int hp_internal_to_full(hp_plan* p, const double2* Fint, double2* Ffull, cudaStream_t s);
+// full layout -> [row][omega], reading only the kept entries of Ff, which may be
+// host memory mapped into the device address space (read in place)
+int hp_full_gather(hp_plan* p, const double2* Ff, double2* Fi, cudaStream_t s);
 // Coefficients of the derivative terms: lie scales the Lie (u) term, gs[i]
 // the gravity component i (coefficient taps, or the density-side term of a
 // density-gravity model when gs[0] or gs[1] is non-zero); b, G, gyro as in hp_model.

@@ -165,6 +165,24 @@ __global__ void k_full_to_int(RowLayout L, const double2* __restrict__ Ff, doubl
   }
 }
 
+// full -> internal reading only the kept entries: block = omega point (grid
+// stride), threads over the kept entries in full-layout order, so that adjacent
+// lanes read adjacent source addresses (the m of one (l, n)) and nothing else
+// of the omega slice is touched.  Ff may be page-locked host memory mapped into
+// the device address space: only the kept entries (a fifth of the full layout
+// for real plans) then cross the bus.  Ff carries no __restrict__ qualifier so
+// that its loads stay on the ordinary global path.
+__global__ void k_full_gather(const int2* __restrict__ fg, int nrows, long long Dfull, long long nx,
+                              const double2* Ff, double2* __restrict__ Fi) {
+  for (long long w = blockIdx.x; w < nx; w += gridDim.x) {
+    const double2* src = Ff + Dfull * w;
+    for (int e = threadIdx.x; e < nrows; e += blockDim.x) {
+      const int2 g = fg[e];
+      Fi[(long long)g.y * nx + w] = src[g.x];
+    }
+  }
+}
+
 __device__ __forceinline__ long long mirror_w(long long w, int N, int ndim) {
   long long r = 0, mul = 1;
   for (int a = 0; a < ndim; ++a) {
@@ -222,6 +240,17 @@ int hp_full_to_internal(hp_plan* p, const double2* Ff, double2* Fi, cudaStream_t
   return HP_OK;
 }
 
+int hp_full_gather(hp_plan* p, const double2* Ff, double2* Fi, cudaStream_t s) {
+  const long long Dfull = (long long)p->D * p->D * (p->lmax + 1);
+  // every block resident at once (8 per SM at 256 threads), each walking
+  // omega points
+  const unsigned g = (unsigned)std::min<long long>(p->nx, 148LL * 8);
+  ProfScope _ps(p, "layout", s);
+  k_full_gather<<<g, 256, 0, s>>>(p->fgather, (int)p->nrows, Dfull, p->nx, Ff, Fi);
+  HP_CUDA_TRY(cudaGetLastError());
+  return HP_OK;
+}
+
 int hp_internal_to_full(hp_plan* p, const double2* Fi, double2* Ff, cudaStream_t s) {
   const int D = p->D;
   const long long Dfull = (long long)D * D * (p->lmax + 1);
@@ -251,6 +280,22 @@ int hp_tables_build(hp_plan* p) {
   HP_CUDA_TRY(hp_dev_alloc(&p->seg, sizeof(int) * p->h_seg.size()));
   HP_CUDA_TRY(cudaMemcpy(p->rows, p->h_rows.data(), sizeof(char4) * p->nrows, cudaMemcpyHostToDevice));
   HP_CUDA_TRY(cudaMemcpy(p->seg, p->h_seg.data(), sizeof(int) * p->h_seg.size(), cudaMemcpyHostToDevice));
+  // kept entries in full-layout order (m fastest, then n, then l), for the
+  // gather that reads only them (k_full_gather)
+  {
+    std::vector<int2> fg;
+    fg.reserve((size_t)p->nrows);
+    for (int l = 0; l <= lmax; ++l)
+      for (int n = -l; n <= l; ++n)
+        for (int m = std::max(-l, p->m_lo); m <= l; ++m) {
+          const int fi = (m + lmax) + D * (n + lmax) + D * D * l;
+          const int row = p->h_seg[(size_t)(m - p->m_lo) * D + n + lmax] + l - std::max(std::abs(m), std::abs(n));
+          fg.push_back(make_int2(fi, row));
+        }
+    if ((long long)fg.size() != p->nrows) { hp_set_error("internal: kept-entry table size"); return HP_ERR_INVALID; }
+    HP_CUDA_TRY(hp_dev_alloc(&p->fgather, sizeof(int2) * fg.size()));
+    HP_CUDA_TRY(cudaMemcpy(p->fgather, fg.data(), sizeof(int2) * fg.size(), cudaMemcpyHostToDevice));
+  }
 
   std::vector<double> fact(2 * lmax + 2, 1.0);
   for (int k = 1; k < (int)fact.size(); ++k) fact[k] = fact[k - 1] * k;

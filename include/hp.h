@@ -13,7 +13,13 @@
  *   f  (2B, 2B, 2B, 2Bx, 2Bx[, 2Bx])                real (or complex), f(alpha, beta, gamma, i, j, k)
  *   MR (2lmax+1, 2lmax+1, lmax+1, n)                complex
  * with lmax = B-1.  `mem` says where a pointer lives (HP_DEVICE or HP_HOST);
- * host pointers are staged through the plan's device workspace.
+ * host pointers are staged through the plan's device workspace.  A host F
+ * input that is 16-byte aligned and page-locked and mapped into the device
+ * address space over its whole extent (e.g. cudaHostAlloc / cudaMallocHost, or
+ * a torch pin_memory tensor) is instead read in place by the layout kernel,
+ * which reads only the entries the plan keeps (|m|, |n| <= l, and m >= 0 for
+ * HP_REAL: about a fifth of the full array at B = 15); hp_host_read_in_place
+ * tells which.  Either way the call returns after the input has been read.
  */
 #ifndef HP_H
 #define HP_H
@@ -92,6 +98,11 @@ typedef struct {
 int hp_plan_create(hp_plan** plan, int B, int Bx, int ndim, int precision, int symmetry);
 int hp_plan_destroy(hp_plan* plan);
 int hp_plan_get_info(const hp_plan* plan, hp_plan_info_t* info);
+/* *in_place = 1 when a host F input of `bytes` bytes at `ptr` is read in place
+ * (16-byte aligned, page-locked and mapped into the current device's address
+ * space at its first and last byte), 0 when it is copied whole to the device
+ * first. */
+int hp_host_read_in_place(const void* ptr, long long bytes, int* in_place);
 /* Stream for every launch of this plan (a cudaStream_t; NULL = legacy default). */
 int hp_plan_set_stream(hp_plan* plan, void* cuda_stream);
 const char* hp_last_error(void);
