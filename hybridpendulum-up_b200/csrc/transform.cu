@@ -63,17 +63,25 @@ __global__ void __launch_bounds__(128) k_wplane(const c2<Tin>* __restrict__ in, 
   const int np = (int)min((long long)PPB, nplanes - pl0);
   const int tot = np * N * N;
   const c2<Tin>* src = in + pl0 * N * N;
-  for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
-    C v[4];
+  if constexpr (sizeof(Tin) == sizeof(T)) {
+    // no conversion: the block's whole run is in flight at once (cp.async,
+    // no register round trip)
+    for (int e = threadIdx.x; e < tot; e += blockDim.x)
+      cp_async<sizeof(C)>(sm + (e / (N * N)) * PS + ((e / N) % N) * (N + 1) + e % N, src + e, true);
+    cp_async_wait_all();
+  } else {
+    for (int e0 = threadIdx.x; e0 < tot; e0 += 4 * blockDim.x) {
+      C v[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int e = e0 + u * blockDim.x;
-      v[u] = e < tot ? cvt<C, c2<Tin>>(src[e]) : czero<C>();
-    }
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        v[u] = e < tot ? cvt<C, c2<Tin>>(src[e]) : czero<C>();
+      }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int e = e0 + u * blockDim.x;
-      if (e < tot) sm[(e / (N * N)) * PS + ((e / N) % N) * (N + 1) + e % N] = v[u];
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < tot) sm[(e / (N * N)) * PS + ((e / N) % N) * (N + 1) + e % N] = v[u];
+      }
     }
   }
   __syncthreads();
