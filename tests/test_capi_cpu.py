@@ -58,6 +58,19 @@ def test_device_budget_and_guard_arguments(hp):
     assert lib.hp_collision_create_from_tables(None, 0, 1, None, None, None, None, 1, None) == hp.HP_ERR_INVALID
 
 
+def test_host_read_in_place_arguments(hp):
+    lib = hp._lib
+    r = ctypes.c_int(-1)
+    a = np.zeros(16, np.complex128)
+    assert lib.hp_host_read_in_place(None, 16, ctypes.byref(r)) == hp.HP_ERR_INVALID
+    assert lib.hp_host_read_in_place(ctypes.c_void_p(a.ctypes.data), 0, ctypes.byref(r)) == hp.HP_ERR_INVALID
+    assert lib.hp_host_read_in_place(ctypes.c_void_p(a.ctypes.data), a.nbytes, None) == hp.HP_ERR_INVALID
+    # pageable memory is never read in place (copied whole), with or without a device
+    assert lib.hp_host_read_in_place(ctypes.c_void_p(a.ctypes.data), a.nbytes, ctypes.byref(r)) == hp.HP_OK
+    assert r.value == 0
+    assert hp.host_read_in_place(a) is False
+
+
 def test_tune_cache_file_round_trip(hp, tmp_path):
     """The autotuner's cache file format: lines read back and written again
     unchanged; malformed lines are reported."""
